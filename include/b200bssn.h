@@ -1,0 +1,140 @@
+/* b200bssn -- B200-native BSSN right-hand side for Dendro octree blocks.
+ *
+ * C ABI of the library (libb200bssn.so).  Plain pointers and sizes only.
+ *
+ * The reference interface this replaces is the per-block C++ entry point
+ *
+ *   void bssnrhs(double **uzipVarsRHS, const double **uZipVars,
+ *                const unsigned int &offset, const double *ptmin, const double *ptmax,
+ *                const unsigned int *sz, const unsigned int &bflag);
+ *                                              (bssn/include/rhs.h:33-36,
+ *                                               bssn/src/rhs.cpp:80-388)
+ *
+ * and the block loop around it, bssnRHS (bssn/src/rhs.cpp:7-70).  Variables are
+ * the 24 BSSN fields in the reference's VAR order (bssn/include/grDef.h:31); each
+ * block is sz[0]*sz[1]*sz[2] contiguous doubles at `offset` in every variable
+ * array, x fastest (IDX(i,j,k) = i + nx*(j + ny*k), bssn/include/derivs.h:8), with
+ * a 3-point ghost layer; ptmin/ptmax are the ghost-inclusive physical corners and
+ * h = (ptmax-ptmin)/(sz-1) (bssn/src/rhs.cpp:144-146); bflag bits 0..5 mark the
+ * faces LEFT,RIGHT,DOWN,UP,BACK,FRONT (bssn/include/def.h:13-18) that get
+ * one-sided stencils and Sommerfeld values.  Only the interior [3,n-3)^3 of the
+ * right-hand side is written.
+ *
+ * Every function returns 0 (B200BSSN_OK) or a negative error code; nothing
+ * aborts the caller.  A context owns its CUDA stream and device buffers; calls on
+ * one context must not overlap (use one context per host thread).
+ */
+#ifndef B200BSSN_H
+#define B200BSSN_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define B200BSSN_NUM_VARS 24
+
+enum b200bssn_status {
+  B200BSSN_OK = 0,
+  B200BSSN_ERR_INVALID_ARGUMENT = -1, /* null pointer, bad size, bad flag */
+  B200BSSN_ERR_BLOCK_TOO_SMALL = -2,  /* an interior extent below 7 points */
+  B200BSSN_ERR_CUDA = -3,             /* a CUDA runtime call failed; see b200bssn_last_error */
+  B200BSSN_ERR_OUT_OF_MEMORY = -4,    /* device allocation failed */
+  B200BSSN_ERR_NO_DEVICE = -5,        /* no usable sm_100 device */
+  B200BSSN_ERR_NONFINITE = -6,        /* the NaN/Inf guard found a non-finite RHS value */
+  B200BSSN_ERR_TIMEOUT = -7,          /* a bounded device wait gave up */
+  B200BSSN_ERR_SIZE_LIMIT = -8        /* request exceeds a documented fixed limit */
+};
+
+/* Arithmetic of the per-point algebra. */
+enum b200bssn_precision {
+  B200BSSN_FP64 = 0,  /* everything in FP64 (the reference's arithmetic) */
+  B200BSSN_MIXED = 1  /* FP64 state, FP64 stencils and KO, FP32 algebra */
+};
+
+/* What happens to the ghost points of the RHS arrays in the host batch call. */
+enum b200bssn_ghost_policy {
+  B200BSSN_GHOSTS_PRESERVE = 0, /* untouched, as the reference leaves them */
+  B200BSSN_GHOSTS_ZERO = 1      /* set to 0 (Dendro's zip reads interior points only) */
+};
+
+/* Solver parameters: the bssn:: globals that bssnrhs reads
+ * (bssn/src/parameters.cpp:99-109), plus the engine's own switches. */
+typedef struct b200bssn_params {
+  uint32_t lambda[4];      /* bssn::BSSN_LAMBDA                           */
+  double lambda_f[2];      /* bssn::BSSN_LAMBDA_F                         */
+  double eta_const;        /* bssn::ETA_CONST                             */
+  double eta_r0;           /* bssn::ETA_R0                                */
+  double eta_damping_exp;  /* bssn::ETA_DAMPING_EXP                       */
+  double ko_sigma;         /* bssn::KO_DISS_SIGMA                         */
+  uint32_t precision;      /* enum b200bssn_precision                     */
+  uint32_t ghost_policy;   /* enum b200bssn_ghost_policy (host batch only) */
+} b200bssn_params;
+
+/* Fills `p` with the reference defaults (bssn/src/parameters.cpp:99-109). */
+void b200bssn_default_params(b200bssn_params *p);
+
+/* One octree block (the arguments bssnRHS derives from an ot::Block,
+ * bssn/src/rhs.cpp:43-60). */
+typedef struct b200bssn_block {
+  uint64_t offset;   /* element offset of the block in every variable array */
+  uint32_t sz[3];    /* padded extents, ghost layer of 3 included           */
+  uint32_t bflag;    /* boundary face bits                                  */
+  double pmin[3];    /* ghost-inclusive lower corner                        */
+  double pmax[3];    /* ghost-inclusive upper corner                        */
+} b200bssn_block;
+
+typedef struct b200bssn_ctx b200bssn_ctx;
+typedef struct b200bssn_plan b200bssn_plan;
+
+/* Context on CUDA device `device` (its own non-blocking stream). */
+int b200bssn_create(b200bssn_ctx **ctx, int device);
+int b200bssn_destroy(b200bssn_ctx *ctx);
+/* The context's stream as an opaque handle (a cudaStream_t). */
+void *b200bssn_stream(b200bssn_ctx *ctx);
+/* Text of the last CUDA error seen by this context (empty if none). */
+const char *b200bssn_last_error(b200bssn_ctx *ctx);
+const char *b200bssn_status_string(int status);
+
+/* Drop-in for bssnrhs (bssn/include/rhs.h:33-36): one block, HOST arrays.
+ * rhs[v] and u[v] (v < 24) are the caller's zipped arrays; the block's slice is
+ * copied to the device, evaluated, and its interior copied back.  Blocks until
+ * the result is in `rhs`. */
+int b200bssn_rhs(b200bssn_ctx *ctx, double *const *rhs, const double *const *u,
+                 uint32_t offset, const double *pmin, const double *pmax,
+                 const uint32_t *sz, uint32_t bflag, const b200bssn_params *prm);
+
+/* Work plan for a fixed block list: descriptors, tiles and the derivative
+ * scratch live on the device.  Build once, evaluate many times (RK stages).
+ * `chunk_points` bounds the interior points evaluated per kernel pair (and so the
+ * scratch: 1296 bytes per point in FP64, 744 in MIXED); 0 picks the default. */
+int b200bssn_plan_create(b200bssn_ctx *ctx, const b200bssn_block *blocks, uint32_t nblocks,
+                         uint32_t precision, uint64_t chunk_points, b200bssn_plan **plan);
+int b200bssn_plan_destroy(b200bssn_plan *plan);
+/* Interior points covered by a plan, and the number of kernel launches one
+ * evaluation issues. */
+uint64_t b200bssn_plan_points(const b200bssn_plan *plan);
+uint32_t b200bssn_plan_launches(const b200bssn_plan *plan);
+
+/* Batched right-hand side on DEVICE arrays (the bssnRHS block loop,
+ * bssn/src/rhs.cpp:41-68).  rhs_dev[v]/u_dev[v] are device pointers to the
+ * zipped arrays.  Asynchronous on `stream` (NULL: the context stream); no
+ * allocation, so it can be captured in a CUDA graph. prm->precision must match
+ * the plan's. */
+int b200bssn_rhs_plan_device(b200bssn_plan *plan, double *const *rhs_dev,
+                             const double *const *u_dev, const b200bssn_params *prm,
+                             void *stream);
+
+/* Batched right-hand side on HOST arrays: uploads the plan's span of every
+ * variable, evaluates, downloads the result (ghost handling per
+ * prm->ghost_policy).  `n_elems` is the length of each host array.  Blocks until
+ * done. */
+int b200bssn_rhs_plan_host(b200bssn_plan *plan, double *const *rhs, const double *const *u,
+                           uint64_t n_elems, const b200bssn_params *prm);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* B200BSSN_H */

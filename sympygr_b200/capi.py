@@ -1,0 +1,242 @@
+"""ctypes binding of the C ABI in include/b200bssn.h (libb200bssn.so).
+
+This is the Python-side mirror of the reference's per-block entry point
+``bssnrhs(uzipVarsRHS, uZipVars, offset, ptmin, ptmax, sz, bflag)``
+(bssn/include/rhs.h:33-36) and of its block loop ``bssnRHS``
+(bssn/src/rhs.cpp:7-70).  There is no fallback: if the CUDA library is missing or
+no sm_100 device is present, every call raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Sequence
+
+import numpy as np
+
+from .workloads import Block
+
+NUM_VARS = 24
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "lib", "libb200bssn.so")
+
+FP64 = 0
+MIXED = 1
+GHOSTS_PRESERVE = 0
+GHOSTS_ZERO = 1
+
+STATUS = {
+    0: "ok", -1: "invalid argument", -2: "block interior below 7 points", -3: "CUDA runtime error",
+    -4: "device out of memory", -5: "no usable sm_100 device", -6: "non-finite right-hand side",
+    -7: "bounded device wait timed out", -8: "request exceeds a fixed size limit",
+}
+
+
+class B200BssnError(RuntimeError):
+    def __init__(self, code: int, what: str, detail: str = ""):
+        self.code = code
+        msg = f"{what}: {STATUS.get(code, code)}"
+        if detail:
+            msg += f" ({detail})"
+        super().__init__(msg)
+
+
+class Params(ctypes.Structure):
+    """``b200bssn_params``: the bssn:: globals bssnrhs reads
+    (bssn/src/parameters.cpp:99-109) plus precision and ghost policy."""
+
+    _fields_ = [
+        ("lambda_", ctypes.c_uint32 * 4),
+        ("lambda_f", ctypes.c_double * 2),
+        ("eta_const", ctypes.c_double),
+        ("eta_r0", ctypes.c_double),
+        ("eta_damping_exp", ctypes.c_double),
+        ("ko_sigma", ctypes.c_double),
+        ("precision", ctypes.c_uint32),
+        ("ghost_policy", ctypes.c_uint32),
+    ]
+
+    @classmethod
+    def make(cls, lambda_=(1, 1, 1, 1), lambda_f=(1.0, 0.0), eta_const=2.0, eta_r0=50.0,
+             eta_damping_exp=1.0, ko_sigma=0.01, precision=FP64, ghost_policy=GHOSTS_PRESERVE):
+        p = cls()
+        for i in range(4):
+            p.lambda_[i] = int(lambda_[i])
+        p.lambda_f[0], p.lambda_f[1] = float(lambda_f[0]), float(lambda_f[1])
+        p.eta_const = eta_const
+        p.eta_r0 = eta_r0
+        p.eta_damping_exp = eta_damping_exp
+        p.ko_sigma = ko_sigma
+        p.precision = precision
+        p.ghost_policy = ghost_policy
+        return p
+
+
+class BlockC(ctypes.Structure):
+    """``b200bssn_block`` (bssn/src/rhs.cpp:43-60 derives these from an ot::Block)."""
+
+    _fields_ = [
+        ("offset", ctypes.c_uint64),
+        ("sz", ctypes.c_uint32 * 3),
+        ("bflag", ctypes.c_uint32),
+        ("pmin", ctypes.c_double * 3),
+        ("pmax", ctypes.c_double * 3),
+    ]
+
+
+_lib = None
+
+# (name, restype, argtypes) of every symbol declared in include/b200bssn.h
+_P = ctypes.c_void_p
+SIGNATURES = [
+    ("b200bssn_default_params", None, [ctypes.POINTER(Params)]),
+    ("b200bssn_create", ctypes.c_int, [ctypes.POINTER(_P), ctypes.c_int]),
+    ("b200bssn_destroy", ctypes.c_int, [_P]),
+    ("b200bssn_stream", _P, [_P]),
+    ("b200bssn_last_error", ctypes.c_char_p, [_P]),
+    ("b200bssn_status_string", ctypes.c_char_p, [ctypes.c_int]),
+    ("b200bssn_rhs", ctypes.c_int, [_P, _P, _P, ctypes.c_uint32, ctypes.POINTER(ctypes.c_double),
+                                    ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_uint32),
+                                    ctypes.c_uint32, ctypes.POINTER(Params)]),
+    ("b200bssn_plan_create", ctypes.c_int, [_P, ctypes.POINTER(BlockC), ctypes.c_uint32,
+                                            ctypes.c_uint32, ctypes.c_uint64, ctypes.POINTER(_P)]),
+    ("b200bssn_plan_destroy", ctypes.c_int, [_P]),
+    ("b200bssn_plan_points", ctypes.c_uint64, [_P]),
+    ("b200bssn_plan_launches", ctypes.c_uint32, [_P]),
+    ("b200bssn_rhs_plan_device", ctypes.c_int, [_P, _P, _P, ctypes.POINTER(Params), _P]),
+    ("b200bssn_rhs_plan_host", ctypes.c_int, [_P, _P, _P, ctypes.c_uint64, ctypes.POINTER(Params)]),
+]
+
+
+def load(path: str = LIB_PATH):
+    """Load libb200bssn.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FileNotFoundError(
+            f"{path} is missing: build it with `python -m sympygr_b200.build` (no CPU fallback)")
+    lib = ctypes.CDLL(path)
+    for name, res, args in SIGNATURES:
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _check(rc: int, what: str, ctx=None):
+    if rc != 0:
+        detail = ""
+        if ctx is not None and ctx.handle:
+            detail = (load().b200bssn_last_error(ctx.handle) or b"").decode()
+        raise B200BssnError(rc, what, detail)
+
+
+def _ptr_table(arrays: Sequence) -> ctypes.Array:
+    """24 raw pointers from numpy arrays or torch tensors (data pointer only)."""
+    if len(arrays) != NUM_VARS:
+        raise ValueError("need 24 variable arrays")
+    ptrs = []
+    for a in arrays:
+        if isinstance(a, np.ndarray):
+            if a.dtype != np.float64 or not a.flags.c_contiguous:
+                raise ValueError("variable arrays must be contiguous float64")
+            ptrs.append(a.ctypes.data)
+        elif isinstance(a, int):
+            ptrs.append(a)
+        else:  # torch tensor
+            if str(a.dtype) != "torch.float64" or not a.is_contiguous():
+                raise ValueError("variable tensors must be contiguous float64")
+            ptrs.append(a.data_ptr())
+    return (ctypes.c_void_p * NUM_VARS)(*ptrs)
+
+
+class Context:
+    """``b200bssn_ctx``: a device, its stream and per-context buffers."""
+
+    def __init__(self, device: int = 0):
+        lib = load()
+        h = ctypes.c_void_p()
+        _check(lib.b200bssn_create(ctypes.byref(h), device), "b200bssn_create")
+        self.handle = h
+        self.device = device
+
+    @property
+    def stream(self) -> int:
+        return load().b200bssn_stream(self.handle) or 0
+
+    def close(self):
+        if self.handle:
+            load().b200bssn_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def bssnrhs(self, rhs, u, offset: int, pmin, pmax, sz, bflag: int, params: Params):
+        """Drop-in for the reference's ``bssnrhs`` on HOST arrays (24 float64
+        arrays each for rhs and u).  Writes the interior of the block in `rhs`."""
+        lib = load()
+        pm = (ctypes.c_double * 3)(*pmin)
+        px = (ctypes.c_double * 3)(*pmax)
+        s = (ctypes.c_uint32 * 3)(*sz)
+        _check(lib.b200bssn_rhs(self.handle, _ptr_table(rhs), _ptr_table(u), int(offset), pm, px,
+                                s, int(bflag), ctypes.byref(params)), "b200bssn_rhs", self)
+
+
+class Plan:
+    """``b200bssn_plan``: descriptors and scratch for a fixed block list."""
+
+    def __init__(self, ctx: Context, blocks: Sequence[Block], precision: int = FP64,
+                 chunk_points: int = 0):
+        lib = load()
+        arr = (BlockC * len(blocks))()
+        for i, b in enumerate(blocks):
+            arr[i].offset = b.offset
+            for a in range(3):
+                arr[i].sz[a] = b.sz[a]
+                arr[i].pmin[a] = b.pmin[a]
+                arr[i].pmax[a] = b.pmax[a]
+            arr[i].bflag = b.bflag
+        h = ctypes.c_void_p()
+        _check(lib.b200bssn_plan_create(ctx.handle, arr, len(blocks), precision, chunk_points,
+                                        ctypes.byref(h)), "b200bssn_plan_create", ctx)
+        self.ctx = ctx
+        self.handle = h
+        self.precision = precision
+
+    @property
+    def points(self) -> int:
+        return int(load().b200bssn_plan_points(self.handle))
+
+    @property
+    def launches(self) -> int:
+        return int(load().b200bssn_plan_launches(self.handle))
+
+    def rhs_device(self, rhs, u, params: Params, stream: int = 0):
+        """Batched RHS on device arrays (torch CUDA tensors or raw pointers);
+        asynchronous on `stream` (0: the context stream)."""
+        _check(load().b200bssn_rhs_plan_device(self.handle, _ptr_table(rhs), _ptr_table(u),
+                                               ctypes.byref(params), ctypes.c_void_p(stream or None)),
+               "b200bssn_rhs_plan_device", self.ctx)
+
+    def rhs_host(self, rhs, u, n_elems: int, params: Params):
+        """Batched RHS on host arrays (H2D, evaluate, D2H; blocks until done)."""
+        _check(load().b200bssn_rhs_plan_host(self.handle, _ptr_table(rhs), _ptr_table(u),
+                                             int(n_elems), ctypes.byref(params)),
+               "b200bssn_rhs_plan_host", self.ctx)
+
+    def close(self):
+        if self.handle:
+            load().b200bssn_plan_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

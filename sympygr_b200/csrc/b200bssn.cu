@@ -1,0 +1,487 @@
+// Host side of libb200bssn: contexts, work plans and the C ABI declared in
+// include/b200bssn.h.  The kernels are in rhs_kernels.cuh.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "b200bssn.h"
+#include "rhs_kernels.cuh"
+
+using namespace b200bssn;
+
+struct b200bssn_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string last_error;
+  // single-block drop-in path
+  double* blk_u = nullptr;    // [24][npad]
+  double* blk_rhs = nullptr;  // [24][npad]
+  size_t blk_cap = 0;         // npad capacity
+  b200bssn_plan* blk_plan = nullptr;
+  uint32_t blk_sz[3] = {0, 0, 0};
+  uint32_t blk_precision = 0xffffffffu;
+};
+
+struct ChunkRec {
+  int32_t tile_begin, tile_count;
+  int32_t range_begin, range_count;
+  int64_t points;
+};
+
+struct b200bssn_plan {
+  b200bssn_ctx* ctx = nullptr;
+  uint32_t precision = 0;
+  std::vector<BlockDev> blocks;
+  std::vector<UnitDev> units;
+  std::vector<TileDev> tiles;
+  std::vector<RangeDev> ranges;
+  std::vector<ChunkRec> chunks;
+  uint64_t points = 0;
+  int64_t cap = 0;
+  uint64_t span_lo = 0, span_hi = 0;  // element range touched in the variable arrays
+  // device
+  void* desc = nullptr;  // blocks | units | tiles | ranges
+  BlockDev* d_blocks = nullptr;
+  UnitDev* d_units = nullptr;
+  TileDev* d_tiles = nullptr;
+  RangeDev* d_ranges = nullptr;
+  void* dscr = nullptr;
+  double* koscr = nullptr;
+  // host-batch staging (allocated on first host call)
+  double* st_u = nullptr;
+  double* st_rhs = nullptr;
+  uint64_t st_len = 0;
+};
+
+namespace {
+
+int fail_cuda(b200bssn_ctx* ctx, cudaError_t e, const char* what) {
+  if (ctx) {
+    ctx->last_error = std::string(what) + ": " + cudaGetErrorString(e);
+  }
+  return e == cudaErrorMemoryAllocation ? B200BSSN_ERR_OUT_OF_MEMORY : B200BSSN_ERR_CUDA;
+}
+
+#define CK(ctx, call)                                   \
+  do {                                                  \
+    cudaError_t e_ = (call);                            \
+    if (e_ != cudaSuccess) return fail_cuda(ctx, e_, #call); \
+  } while (0)
+
+constexpr int64_t kDefaultChunkPoints = int64_t(1) << 21;
+
+bool params_ok(const b200bssn_params* p) {
+  return p && (p->precision == B200BSSN_FP64 || p->precision == B200BSSN_MIXED) &&
+         (p->ghost_policy == B200BSSN_GHOSTS_PRESERVE || p->ghost_policy == B200BSSN_GHOSTS_ZERO);
+}
+
+int launch_plan(b200bssn_plan* P, double* const* rhs, const double* const* u,
+                const b200bssn_params* prm, cudaStream_t s) {
+  b200bssn_ctx* ctx = P->ctx;
+  DerivArgs da;
+  AlgebraArgs aa;
+  for (int v = 0; v < kNumVars; ++v) {
+    da.u[v] = u[v];
+    aa.u[v] = u[v];
+    aa.rhs[v] = rhs[v];
+  }
+  da.blocks = aa.blocks = P->d_blocks;
+  da.units = aa.units = P->d_units;
+  da.tiles = P->d_tiles;
+  aa.ranges = P->d_ranges;
+  da.dscr = P->dscr;
+  aa.dscr = P->dscr;
+  da.koscr = P->koscr;
+  aa.koscr = P->koscr;
+  da.cap = aa.cap = P->cap;
+  aa.prm64 = {(double)prm->lambda[0], (double)prm->lambda[1], (double)prm->lambda[2],
+              (double)prm->lambda[3], prm->lambda_f[0], prm->lambda_f[1]};
+  aa.prm32 = {(float)prm->lambda[0], (float)prm->lambda[1], (float)prm->lambda[2],
+              (float)prm->lambda[3], (float)prm->lambda_f[0], (float)prm->lambda_f[1]};
+  aa.eta_const = prm->eta_const;
+  aa.eta_r0 = prm->eta_r0;
+  aa.eta_damping_exp = prm->eta_damping_exp;
+  aa.ko_sigma = prm->ko_sigma;
+  const bool mixed = P->precision == B200BSSN_MIXED;
+  for (const ChunkRec& c : P->chunks) {
+    da.tile_base = c.tile_begin;
+    aa.range_base = c.range_begin;
+    dim3 g1(c.tile_count, kNumVars);
+    if (mixed)
+      bssn_derivs_kernel<float><<<g1, kDerivThreads, kDerivSmemBytes, s>>>(da);
+    else
+      bssn_derivs_kernel<double><<<g1, kDerivThreads, kDerivSmemBytes, s>>>(da);
+    CK(ctx, cudaGetLastError());
+    if (mixed)
+      bssn_algebra_kernel<float, float><<<c.range_count, kAlgebraThreads, 0, s>>>(aa);
+    else
+      bssn_algebra_kernel<double, double><<<c.range_count, kAlgebraThreads, 0, s>>>(aa);
+    CK(ctx, cudaGetLastError());
+  }
+  return B200BSSN_OK;
+}
+
+int set_kernel_attributes(b200bssn_ctx* ctx) {
+  CK(ctx, cudaFuncSetAttribute(bssn_derivs_kernel<double>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDerivSmemBytes));
+  CK(ctx, cudaFuncSetAttribute(bssn_derivs_kernel<float>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDerivSmemBytes));
+  return B200BSSN_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void b200bssn_default_params(b200bssn_params* p) {
+  if (!p) return;
+  std::memset(p, 0, sizeof(*p));
+  for (int i = 0; i < 4; ++i) p->lambda[i] = 1;
+  p->lambda_f[0] = 1.0;
+  p->lambda_f[1] = 0.0;
+  p->eta_const = 2.0;
+  p->eta_r0 = 50.0;
+  p->eta_damping_exp = 1.0;
+  p->ko_sigma = 0.01;
+  p->precision = B200BSSN_FP64;
+  p->ghost_policy = B200BSSN_GHOSTS_PRESERVE;
+}
+
+const char* b200bssn_status_string(int s) {
+  switch (s) {
+    case B200BSSN_OK: return "ok";
+    case B200BSSN_ERR_INVALID_ARGUMENT: return "invalid argument";
+    case B200BSSN_ERR_BLOCK_TOO_SMALL: return "block interior below 7 points";
+    case B200BSSN_ERR_CUDA: return "CUDA runtime error";
+    case B200BSSN_ERR_OUT_OF_MEMORY: return "device out of memory";
+    case B200BSSN_ERR_NO_DEVICE: return "no usable sm_100 device";
+    case B200BSSN_ERR_NONFINITE: return "non-finite right-hand side";
+    case B200BSSN_ERR_TIMEOUT: return "bounded device wait timed out";
+    case B200BSSN_ERR_SIZE_LIMIT: return "request exceeds a fixed size limit";
+    default: return "unknown status";
+  }
+}
+
+int b200bssn_create(b200bssn_ctx** out, int device) {
+  if (!out) return B200BSSN_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n) {
+    cudaGetLastError();
+    return B200BSSN_ERR_NO_DEVICE;
+  }
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess || prop.major != 10) {
+    cudaGetLastError();
+    return B200BSSN_ERR_NO_DEVICE;
+  }
+  b200bssn_ctx* ctx = new b200bssn_ctx();
+  ctx->device = device;
+  int rc = B200BSSN_OK;
+  cudaError_t e = cudaSetDevice(device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) rc = fail_cuda(ctx, e, "context setup");
+  if (rc == B200BSSN_OK) rc = set_kernel_attributes(ctx);
+  if (rc != B200BSSN_OK) {
+    b200bssn_destroy(ctx);
+    return rc;
+  }
+  *out = ctx;
+  return B200BSSN_OK;
+}
+
+int b200bssn_destroy(b200bssn_ctx* ctx) {
+  if (!ctx) return B200BSSN_ERR_INVALID_ARGUMENT;
+  cudaSetDevice(ctx->device);
+  if (ctx->blk_plan) b200bssn_plan_destroy(ctx->blk_plan);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  cudaFree(ctx->blk_u);
+  cudaFree(ctx->blk_rhs);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return B200BSSN_OK;
+}
+
+void* b200bssn_stream(b200bssn_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+const char* b200bssn_last_error(b200bssn_ctx* ctx) { return ctx ? ctx->last_error.c_str() : ""; }
+
+int b200bssn_plan_create(b200bssn_ctx* ctx, const b200bssn_block* blocks, uint32_t nblocks,
+                         uint32_t precision, uint64_t chunk_points, b200bssn_plan** out) {
+  if (!ctx || !blocks || !out || nblocks == 0) return B200BSSN_ERR_INVALID_ARGUMENT;
+  if (precision != B200BSSN_FP64 && precision != B200BSSN_MIXED) return B200BSSN_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  CK(ctx, cudaSetDevice(ctx->device));
+  b200bssn_plan* P = new b200bssn_plan();
+  P->ctx = ctx;
+  P->precision = precision;
+  P->span_lo = UINT64_MAX;
+  int64_t max_unit = 0;
+  for (uint32_t b = 0; b < nblocks; ++b) {
+    const b200bssn_block& in = blocks[b];
+    for (int a = 0; a < 3; ++a) {
+      if (in.sz[a] < 13) {
+        delete P;
+        return B200BSSN_ERR_BLOCK_TOO_SMALL;
+      }
+      if (in.sz[a] > 32767 || !(in.pmax[a] > in.pmin[a])) {
+        delete P;
+        return B200BSSN_ERR_INVALID_ARGUMENT;
+      }
+    }
+    if (in.bflag >> 6) {
+      delete P;
+      return B200BSSN_ERR_INVALID_ARGUMENT;
+    }
+    BlockDev d;
+    d.offset = in.offset;
+    d.bflag = in.bflag;
+    for (int a = 0; a < 3; ++a) {
+      d.sz[a] = (int32_t)in.sz[a];
+      d.pmin[a] = in.pmin[a];
+      d.h[a] = (in.pmax[a] - in.pmin[a]) / (in.sz[a] - 1);  // rhs.cpp:144-146
+    }
+    P->blocks.push_back(d);
+    const uint64_t npad = (uint64_t)in.sz[0] * in.sz[1] * in.sz[2];
+    P->span_lo = std::min<uint64_t>(P->span_lo, in.offset);
+    P->span_hi = std::max<uint64_t>(P->span_hi, in.offset + npad);
+    const int64_t I0 = in.sz[0] - 6, I1 = in.sz[1] - 6, I2 = in.sz[2] - 6;
+    if ((uint64_t)I0 * I1 * kTileZ > (uint64_t)INT32_MAX) {
+      delete P;
+      return B200BSSN_ERR_INVALID_ARGUMENT;
+    }
+    for (int64_t k0 = 0; k0 < I2; k0 += kTileZ) {
+      UnitDev u;
+      u.block = (int32_t)b;
+      u.k0 = (int32_t)k0;
+      u.nz = (int32_t)std::min<int64_t>(kTileZ, I2 - k0);
+      u.pad = 0;
+      u.sbase = 0;
+      P->units.push_back(u);
+      max_unit = std::max<int64_t>(max_unit, I0 * I1 * u.nz);
+    }
+    P->points += (uint64_t)(I0 * I1 * I2);
+  }
+  int64_t capacity = chunk_points ? (int64_t)chunk_points : kDefaultChunkPoints;
+  capacity = std::max(capacity, max_unit);
+  // pack units into chunks
+  ChunkRec cur{0, 0, 0, 0, 0};
+  auto flush = [&]() {
+    if (cur.points > 0) {
+      cur.tile_count = (int32_t)P->tiles.size() - cur.tile_begin;
+      cur.range_count = (int32_t)P->ranges.size() - cur.range_begin;
+      P->chunks.push_back(cur);
+      P->cap = std::max<int64_t>(P->cap, cur.points);
+    }
+    cur = ChunkRec{(int32_t)P->tiles.size(), 0, (int32_t)P->ranges.size(), 0, 0};
+  };
+  for (size_t ui = 0; ui < P->units.size(); ++ui) {
+    UnitDev& u = P->units[ui];
+    const BlockDev& B = P->blocks[u.block];
+    const int I0 = B.sz[0] - 6, I1 = B.sz[1] - 6;
+    const int64_t np = (int64_t)I0 * I1 * u.nz;
+    if (cur.points + np > capacity) flush();
+    u.sbase = cur.points;
+    cur.points += np;
+    for (int j0 = 0; j0 < I1; j0 += kTileY)
+      for (int i0 = 0; i0 < I0; i0 += kTileX) {
+        TileDev t;
+        t.unit = (int32_t)ui;
+        t.i0 = (int16_t)i0;
+        t.j0 = (int16_t)j0;
+        t.ex = (int16_t)std::min(kTileX, I0 - i0);
+        t.ey = (int16_t)std::min(kTileY, I1 - j0);
+        P->tiles.push_back(t);
+      }
+    for (int64_t s = 0; s < np; s += kAlgebraThreads) {
+      RangeDev r;
+      r.unit = (int32_t)ui;
+      r.start = (int32_t)s;
+      r.count = (int32_t)std::min<int64_t>(kAlgebraThreads, np - s);
+      P->ranges.push_back(r);
+    }
+  }
+  flush();
+
+  const size_t nb = P->blocks.size() * sizeof(BlockDev), nu = P->units.size() * sizeof(UnitDev),
+               nt = P->tiles.size() * sizeof(TileDev), nr = P->ranges.size() * sizeof(RangeDev);
+  auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
+  const size_t total = al(nb) + al(nu) + al(nt) + al(nr);
+  cudaError_t e = cudaMalloc(&P->desc, total);
+  const size_t st = precision == B200BSSN_MIXED ? sizeof(float) : sizeof(double);
+  if (e == cudaSuccess) e = cudaMalloc(&P->dscr, (size_t)kNumDerivs * P->cap * st);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&P->koscr, (size_t)kNumVars * P->cap * sizeof(double));
+  if (e != cudaSuccess) {
+    int rc = fail_cuda(ctx, e, "plan allocation");
+    b200bssn_plan_destroy(P);
+    return rc;
+  }
+  char* base = static_cast<char*>(P->desc);
+  P->d_blocks = reinterpret_cast<BlockDev*>(base);
+  P->d_units = reinterpret_cast<UnitDev*>(base + al(nb));
+  P->d_tiles = reinterpret_cast<TileDev*>(base + al(nb) + al(nu));
+  P->d_ranges = reinterpret_cast<RangeDev*>(base + al(nb) + al(nu) + al(nt));
+  e = cudaMemcpy(P->d_blocks, P->blocks.data(), nb, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(P->d_units, P->units.data(), nu, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(P->d_tiles, P->tiles.data(), nt, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(P->d_ranges, P->ranges.data(), nr, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    int rc = fail_cuda(ctx, e, "plan upload");
+    b200bssn_plan_destroy(P);
+    return rc;
+  }
+  *out = P;
+  return B200BSSN_OK;
+}
+
+int b200bssn_plan_destroy(b200bssn_plan* P) {
+  if (!P) return B200BSSN_ERR_INVALID_ARGUMENT;
+  if (P->ctx) cudaSetDevice(P->ctx->device);
+  cudaFree(P->desc);
+  cudaFree(P->dscr);
+  cudaFree(P->koscr);
+  cudaFree(P->st_u);
+  cudaFree(P->st_rhs);
+  delete P;
+  return B200BSSN_OK;
+}
+
+uint64_t b200bssn_plan_points(const b200bssn_plan* P) { return P ? P->points : 0; }
+
+uint32_t b200bssn_plan_launches(const b200bssn_plan* P) {
+  return P ? (uint32_t)(2 * P->chunks.size()) : 0;
+}
+
+int b200bssn_rhs_plan_device(b200bssn_plan* P, double* const* rhs_dev, const double* const* u_dev,
+                             const b200bssn_params* prm, void* stream) {
+  if (!P || !rhs_dev || !u_dev || !params_ok(prm)) return B200BSSN_ERR_INVALID_ARGUMENT;
+  if (prm->precision != P->precision) return B200BSSN_ERR_INVALID_ARGUMENT;
+  for (int v = 0; v < kNumVars; ++v)
+    if (!rhs_dev[v] || !u_dev[v]) return B200BSSN_ERR_INVALID_ARGUMENT;
+  cudaStream_t s = stream ? (cudaStream_t)stream : P->ctx->stream;
+  return launch_plan(P, rhs_dev, u_dev, prm, s);
+}
+
+int b200bssn_rhs_plan_host(b200bssn_plan* P, double* const* rhs, const double* const* u,
+                           uint64_t n_elems, const b200bssn_params* prm) {
+  if (!P || !rhs || !u || !params_ok(prm)) return B200BSSN_ERR_INVALID_ARGUMENT;
+  if (prm->precision != P->precision || n_elems < P->span_hi) return B200BSSN_ERR_INVALID_ARGUMENT;
+  for (int v = 0; v < kNumVars; ++v)
+    if (!rhs[v] || !u[v]) return B200BSSN_ERR_INVALID_ARGUMENT;
+  b200bssn_ctx* ctx = P->ctx;
+  CK(ctx, cudaSetDevice(ctx->device));
+  const uint64_t len = P->span_hi - P->span_lo;
+  if (P->st_len < len) {
+    cudaFree(P->st_u);
+    cudaFree(P->st_rhs);
+    P->st_u = P->st_rhs = nullptr;
+    P->st_len = 0;
+    CK(ctx, cudaMalloc((void**)&P->st_u, (size_t)kNumVars * len * sizeof(double)));
+    CK(ctx, cudaMalloc((void**)&P->st_rhs, (size_t)kNumVars * len * sizeof(double)));
+    P->st_len = len;
+  }
+  cudaStream_t s = ctx->stream;
+  const double* ud[kNumVars];
+  double* rd[kNumVars];
+  const size_t bytes = len * sizeof(double);
+  for (int v = 0; v < kNumVars; ++v) {
+    // device arrays are shifted so that element `span_lo` lands at the start
+    ud[v] = P->st_u + (size_t)v * len - P->span_lo;
+    rd[v] = P->st_rhs + (size_t)v * len - P->span_lo;
+    CK(ctx, cudaMemcpyAsync(P->st_u + (size_t)v * len, u[v] + P->span_lo, bytes,
+                            cudaMemcpyHostToDevice, s));
+    if (prm->ghost_policy == B200BSSN_GHOSTS_PRESERVE)
+      CK(ctx, cudaMemcpyAsync(P->st_rhs + (size_t)v * len, rhs[v] + P->span_lo, bytes,
+                              cudaMemcpyHostToDevice, s));
+    else
+      CK(ctx, cudaMemsetAsync(P->st_rhs + (size_t)v * len, 0, bytes, s));
+  }
+  int rc = launch_plan(P, rd, ud, prm, s);
+  if (rc != B200BSSN_OK) return rc;
+  for (int v = 0; v < kNumVars; ++v)
+    CK(ctx, cudaMemcpyAsync(rhs[v] + P->span_lo, P->st_rhs + (size_t)v * len, bytes,
+                            cudaMemcpyDeviceToHost, s));
+  CK(ctx, cudaStreamSynchronize(s));
+  return B200BSSN_OK;
+}
+
+int b200bssn_rhs(b200bssn_ctx* ctx, double* const* rhs, const double* const* u, uint32_t offset,
+                 const double* pmin, const double* pmax, const uint32_t* sz, uint32_t bflag,
+                 const b200bssn_params* prm) {
+  if (!ctx || !rhs || !u || !pmin || !pmax || !sz || !params_ok(prm))
+    return B200BSSN_ERR_INVALID_ARGUMENT;
+  for (int v = 0; v < kNumVars; ++v)
+    if (!rhs[v] || !u[v]) return B200BSSN_ERR_INVALID_ARGUMENT;
+  CK(ctx, cudaSetDevice(ctx->device));
+  b200bssn_block blk;
+  blk.offset = 0;
+  blk.bflag = bflag;
+  for (int a = 0; a < 3; ++a) {
+    blk.sz[a] = sz[a];
+    blk.pmin[a] = pmin[a];
+    blk.pmax[a] = pmax[a];
+  }
+  const size_t npad = (size_t)sz[0] * sz[1] * sz[2];
+  // (re)build the one-block plan when the size or precision changes; otherwise
+  // only the block descriptor (corners, flags) is refreshed.
+  if (!ctx->blk_plan || std::memcmp(ctx->blk_sz, sz, sizeof(ctx->blk_sz)) != 0 ||
+      ctx->blk_precision != prm->precision) {
+    if (ctx->blk_plan) b200bssn_plan_destroy(ctx->blk_plan);
+    ctx->blk_plan = nullptr;
+    int rc = b200bssn_plan_create(ctx, &blk, 1, prm->precision, 0, &ctx->blk_plan);
+    if (rc != B200BSSN_OK) return rc;
+    std::memcpy(ctx->blk_sz, sz, sizeof(ctx->blk_sz));
+    ctx->blk_precision = prm->precision;
+  } else {
+    BlockDev& d = ctx->blk_plan->blocks[0];
+    d.bflag = bflag;
+    for (int a = 0; a < 3; ++a) {
+      d.pmin[a] = pmin[a];
+      d.h[a] = (pmax[a] - pmin[a]) / (sz[a] - 1);
+    }
+    if (bflag >> 6) return B200BSSN_ERR_INVALID_ARGUMENT;
+    CK(ctx, cudaMemcpyAsync(ctx->blk_plan->d_blocks, &d, sizeof(BlockDev), cudaMemcpyHostToDevice,
+                            ctx->stream));
+  }
+  if (ctx->blk_cap < npad) {
+    cudaFree(ctx->blk_u);
+    cudaFree(ctx->blk_rhs);
+    ctx->blk_u = ctx->blk_rhs = nullptr;
+    ctx->blk_cap = 0;
+    CK(ctx, cudaMalloc((void**)&ctx->blk_u, kNumVars * npad * sizeof(double)));
+    CK(ctx, cudaMalloc((void**)&ctx->blk_rhs, kNumVars * npad * sizeof(double)));
+    ctx->blk_cap = npad;
+  }
+  cudaStream_t s = ctx->stream;
+  const double* ud[kNumVars];
+  double* rd[kNumVars];
+  for (int v = 0; v < kNumVars; ++v) {
+    ud[v] = ctx->blk_u + v * npad;
+    rd[v] = ctx->blk_rhs + v * npad;
+    CK(ctx, cudaMemcpyAsync((void*)ud[v], u[v] + offset, npad * sizeof(double),
+                            cudaMemcpyHostToDevice, s));
+  }
+  int rc = launch_plan(ctx->blk_plan, rd, ud, prm, s);
+  if (rc != B200BSSN_OK) return rc;
+  // copy back the interior box only: the reference leaves ghost points untouched
+  const size_t nx = sz[0], ny = sz[1];
+  for (int v = 0; v < kNumVars; ++v) {
+    cudaMemcpy3DParms cp;
+    std::memset(&cp, 0, sizeof(cp));
+    cp.srcPtr = make_cudaPitchedPtr(rd[v], nx * sizeof(double), nx, ny);
+    cp.dstPtr = make_cudaPitchedPtr(rhs[v] + offset, nx * sizeof(double), nx, ny);
+    cp.srcPos = make_cudaPos(3 * sizeof(double), 3, 3);
+    cp.dstPos = cp.srcPos;
+    cp.extent = make_cudaExtent((nx - 6) * sizeof(double), ny - 6, sz[2] - 6);
+    cp.kind = cudaMemcpyDeviceToHost;
+    CK(ctx, cudaMemcpy3DAsync(&cp, s));
+  }
+  CK(ctx, cudaStreamSynchronize(s));
+  return B200BSSN_OK;
+}
+
+}  // extern "C"

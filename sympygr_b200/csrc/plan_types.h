@@ -1,0 +1,50 @@
+// Work-plan descriptors shared by the host planner and the kernels.
+//
+// A plan covers a list of octree blocks.  Each block's interior (sz-6)^3 is cut
+// into z-slabs ("units") of at most kTileZ planes; a unit's points are numbered
+// compactly, x fastest:  lp = (i-3) + I0*((j-3) + I1*(k-3-k0)).  Units are packed
+// into chunks whose total point count fits the derivative scratch; each chunk is
+// evaluated by one derivative launch (one CTA per x-y tile of a unit and per
+// variable) followed by one algebra launch (one CTA per run of consecutive points
+// of a unit).
+#pragma once
+#include <stdint.h>
+
+namespace b200bssn {
+
+constexpr int kNumVars = 24;
+constexpr int kNumDerivs = 138;  // algebra inputs: 72 first + 66 second derivatives
+constexpr int kTileX = 8, kTileY = 8, kTileZ = 8;
+constexpr int kHalo = 4;         // closure rows reach four points inward
+constexpr int kDerivThreads = 256;
+constexpr int kAlgebraThreads = 128;
+
+struct BlockDev {
+  uint64_t offset;   // element offset in every variable array
+  int32_t sz[3];
+  uint32_t bflag;
+  double pmin[3];    // ghost-inclusive corner
+  double h[3];       // (pmax - pmin)/(sz - 1), computed on the host as bssnrhs does
+};
+
+struct UnitDev {
+  int32_t block;
+  int32_t k0;        // first interior plane of the slab (0-based interior index)
+  int32_t nz;        // planes in the slab (<= kTileZ)
+  int32_t pad;
+  int64_t sbase;     // first scratch point of the unit within its chunk
+};
+
+struct TileDev {
+  int32_t unit;
+  int16_t i0, j0;    // interior-relative origin of the x-y tile
+  int16_t ex, ey;    // extents (<= kTileX, kTileY)
+};
+
+struct RangeDev {
+  int32_t unit;
+  int32_t start;     // first compact point index within the unit
+  int32_t count;     // <= kAlgebraThreads
+};
+
+}  // namespace b200bssn

@@ -1,0 +1,390 @@
+#!/usr/bin/env python
+"""Benchmark: batched BSSN right-hand side on B200, mixed precision vs plain FP64.
+
+Workload (one "step" = one RHS evaluation of the whole batch): the octree-like
+two-puncture Brill-Lindquist batch of 3000 blocks, padded sizes 13/21/37/69/135
+(1800/750/300/120/30 blocks), 1.065e8 interior points, KO sigma 0.4, inputs
+resident in HBM (26.7 GB per 24-variable state, far larger than the 126 MB L2, so
+no flush is needed between steps).  `value` is the MIXED-precision throughput
+(FP64 state and stencils, FP32 algebra) in interior Mpoints/s; the plain FP64
+path is timed the same way and reported beside it.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Multi-GPU (torchrun): every rank evaluates its own batch (weak scaling, no
+collective on the data path); time = max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+METRIC = "BSSN RHS Mpoints/s, mixed vs plain FP64 on 1 B200 at <=1e-6 rel err; %roofline"
+UNIT = "Mpoints/s"
+SIGMA = 0.4
+# Algorithmic work per interior point.  Algebra: the CSE'd expression count of the
+# generated device function (sympy count_ops, an FMA counted as 2) plus the KO add
+# (2 per variable) and the eta damping (~10).  Derivatives: 72 first derivatives
+# x 12 flops (6-point stencil, multiply-add each), 33 second derivatives x 14,
+# 33 mixed (a first derivative of a first derivative) x 12, KO 72 x 14.
+ALGEBRA_FLOPS_PER_POINT = 4267 + 48 + 10
+DERIV_FLOPS_PER_POINT = 72 * 12 + 33 * 14 + 33 * 12 + 72 * 14
+MIXED_BAR = 1e-6
+
+
+def _env_int(k, d):
+    try:
+        return int(os.environ.get(k, d))
+    except ValueError:
+        return d
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+        self.t = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+            return
+        self.t = threading.Thread(target=self._read, daemon=True)
+        self.t.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        if self.t:
+            self.t.join(timeout=2)
+        sm, smax, reasons, power = [], None, set(), []
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+                power.append(float(f[3]))
+            except ValueError:
+                continue
+            for name, val in zip(["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                                  "sw_power_cap"], f[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm),
+                "power_w_max": max(power) if power else None}
+
+
+def stratified_blocks(blocks, frac):
+    """A class-proportional subset of a block list (at least one block per class)."""
+    by = {}
+    for b in blocks:
+        by.setdefault(b.sz[0], []).append(b)
+    out = []
+    for n, bl in sorted(by.items()):
+        m = max(1, int(round(len(bl) * frac)))
+        out.extend(bl[:m])
+    return out
+
+
+def cpu_reference_run(u_host, blocks, nthreads):
+    """The reference's own CPU bssnrhs (compiled from its sources, -O3) over a block
+    list in its block-parallel OpenMP loop; returns (seconds, interior points)."""
+    import numpy as np
+
+    from oracle import pyoracle as po
+
+    rhs = np.zeros_like(u_host)
+    prm = po.params(ko_sigma=SIGMA)
+    secs = po.ref_blocks_omp(u_host, rhs, blocks, prm, nthreads=nthreads, flavour="fast")
+    return secs, sum(b.ninterior for b in blocks)
+
+
+def compact_host_batch(blocks):
+    """Host arrays for a block subset, re-offset compactly (numpy generator)."""
+    import numpy as np
+
+    from sympygr_b200 import workloads as wl
+
+    out, off = [], 0
+    for b in blocks:
+        out.append(wl.Block(off, b.sz, b.bflag, b.pmin, b.pmax))
+        off += b.npad
+    u = np.zeros((24, off))
+    punct = [(-4.0, 0.0, 0.0, 0.5), (4.0, 0.0, 0.0, 0.5)]
+    for b in out:
+        x, y, z = wl.coords(b)
+        wl._bl_fields(u, slice(b.offset, b.offset + b.npad), x, y, z, punct)
+    return u, out
+
+
+def reference_arm(args, rank, world):
+    """`--impl reference`: the reference's CPU bssnrhs on this host's cores."""
+    if rank != 0:
+        return None
+    from oracle import pyoracle as po
+    from sympygr_b200 import workloads as wl
+
+    if not po.have_reference("fast"):
+        return {"impl": "reference", "unavailable": "reference build oracle/_ref/libbssn_ref_fast.so missing"}
+    ncores = os.cpu_count() or 1
+    blocks, _ = wl.batch_blocks(seed=0)
+    sample = stratified_blocks(blocks, args.ref_fraction)
+    u, sblocks = compact_host_batch(sample)
+    # big blocks first so the block-parallel loop does not end on a long tail
+    order = sorted(range(len(sblocks)), key=lambda i: -sblocks[i].npad)
+    sblocks = [sblocks[i] for i in order]
+    for _ in range(max(0, min(args.warmup, 1))):
+        cpu_reference_run(u, sblocks, ncores)
+    times, pts = [], 0
+    for _ in range(max(1, min(args.steps, 3))):
+        s, pts = cpu_reference_run(u, sblocks, ncores)
+        times.append(s)
+    t = statistics.median(times)
+    val = pts / t / 1e6
+    sample_desc = (f"{len(sblocks)} of 3000 blocks ({args.ref_fraction:.3g} class-proportional "
+                   f"sample, {pts} interior points) per step; median of {len(times)} steps")
+    return {
+        "metric": METRIC, "value": round(val, 4), "unit": UNIT, "impl": "reference",
+        "n_gpus": world, "steps": len(times), "warmup": min(args.warmup, 1),
+        "ms_per_step": round(t * 1e3, 2), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "two-puncture Brill-Lindquist batch, 3000 blocks 13^3..135^3",
+                   "sample": sample_desc},
+        "cpu_baseline": {"value": round(val, 4), "unit": UNIT, "cores": ncores, "kind": "reference",
+                         "sample": sample_desc},
+        "e2e": {"value": round(val, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--scale", type=float, default=1.0,
+                    help="fraction of the 3000-block batch (1.0 = the benchmark workload)")
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--ref-fraction", type=float, default=0.1)
+    ap.add_argument("--chunk-points", type=int, default=0)
+    args = ap.parse_args()
+
+    world = _env_int("WORLD_SIZE", 1)
+    rank = _env_int("RANK", 0)
+    local_rank = _env_int("LOCAL_RANK", 0)
+
+    if args.impl == "reference":
+        out = reference_arm(args, rank, world)
+        if out is not None:
+            print(json.dumps(out), flush=True)
+        return
+
+    import numpy as np
+    import torch
+
+    import sympygr_b200 as sg
+    from sympygr_b200 import capi
+    from sympygr_b200 import workloads as wl
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    counts = tuple(max(1, int(round(c * args.scale))) for c in wl.BATCH_COUNTS)
+    u, blocks = wl.two_puncture_batch_torch(wl.BATCH_SIZES, counts, seed=rank, device="cuda")
+    rhs = torch.zeros_like(u)
+    ctx = sg.Context(local_rank)
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    plans = {p: sg.Plan(ctx, blocks, p, args.chunk_points) for p in (sg.FP64, sg.MIXED)}
+    params = {p: sg.Params.make(ko_sigma=SIGMA, precision=p) for p in (sg.FP64, sg.MIXED)}
+    npts = plans[sg.FP64].points
+    U, R = list(u), list(rhs)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def timed(prec, k):
+        barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(k):
+            plans[prec].rhs_device(R, U, params[prec])
+        e1.record(stream)
+        e1.synchronize()
+        torch.cuda.synchronize()
+        barrier()
+        ms = e0.elapsed_time(e1)
+        if dist is not None:
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = t.item()
+        return ms / k
+
+    for prec in (sg.MIXED, sg.FP64):
+        for _ in range(args.warmup):
+            plans[prec].rhs_device(R, U, params[prec])
+    torch.cuda.synchronize()
+
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    ms_mixed = timed(sg.MIXED, args.steps)
+    clock_info = clocks.stop()
+    ms_fp64 = timed(sg.FP64, args.steps)
+
+    # accuracy of the headline path: mixed vs FP64 on the same inputs
+    plans[sg.FP64].rhs_device(R, U, params[sg.FP64])
+    torch.cuda.synchronize()
+    ref64 = rhs.clone()
+    plans[sg.MIXED].rhs_device(R, U, params[sg.MIXED])
+    torch.cuda.synchronize()
+    scale = ref64.abs().amax(dim=1)
+    err = ((rhs - ref64).abs().amax(dim=1) / scale.clamp_min(1e-300)).where(scale > 0, torch.zeros_like(scale))
+    mixed_max_rel = float(err.max().item())
+    del ref64
+
+    # per-kernel device time of one evaluation (events between launches)
+    prof = {}
+    for prec in (sg.MIXED, sg.FP64):
+        d_ms, a_ms = plans[prec].profile(R, U, params[prec])
+        prof[prec] = (d_ms, a_ms)
+    peak64 = capi.fma_peak_tflops(local_rank, sg.FP64)
+    peak32 = capi.fma_peak_tflops(local_rank, sg.MIXED)
+
+    launches = plans[sg.MIXED].launches * args.steps
+    total_pts = npts * world
+    val_mixed = total_pts / (ms_mixed * 1e-3) / 1e6
+    val_fp64 = total_pts / (ms_fp64 * 1e-3) / 1e6
+
+    d_ms, a_ms = prof[sg.MIXED]
+    alg_tf = ALGEBRA_FLOPS_PER_POINT * npts / (a_ms * 1e-3) / 1e12
+    d64, a64 = prof[sg.FP64]
+    alg64_tf = ALGEBRA_FLOPS_PER_POINT * npts / (a64 * 1e-3) / 1e12
+
+    # end to end through the host API: H2D of the state, evaluate, D2H of the RHS
+    e2e = None
+    if not args.no_e2e:
+        span = max(b.offset + b.npad for b in blocks)
+        u_h = u.to("cpu").pin_memory() if True else None
+        del rhs, u
+        U = R = None
+        torch.cuda.empty_cache()
+        r_h = torch.empty_like(u_h).pin_memory()
+        p_host = sg.Params.make(ko_sigma=SIGMA, precision=sg.MIXED, ghost_policy=sg.GHOSTS_ZERO)
+        UH, RH = [t.data_ptr() for t in u_h], [t.data_ptr() for t in r_h]
+        plans[sg.MIXED].rhs_host(RH, UH, span, p_host)  # warm-up (allocates staging)
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.e2e_steps):
+            plans[sg.MIXED].rhs_host(RH, UH, span, p_host)
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / args.e2e_steps
+        if dist is not None:
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = t.item()
+        nbytes = 24 * span * 8
+        e2e = {"value": round(total_pts / (ms * 1e-3) / 1e6, 3), "unit": UNIT,
+               "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
+               "ms_per_step": round(ms, 2), "steps": args.e2e_steps,
+               "api": "b200bssn_rhs_plan_host (pinned host arrays, ghosts zeroed)"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            from oracle import pyoracle as po
+
+            if po.have_reference("fast"):
+                sample = stratified_blocks(blocks, args.ref_fraction)
+                uh, sb = compact_host_batch(sample)
+                sb = [sb[i] for i in sorted(range(len(sb)), key=lambda i: -sb[i].npad)]
+                secs, pts = cpu_reference_run(uh, sb, os.cpu_count() or 1)
+                cpu = {"value": round(pts / secs / 1e6, 4), "unit": UNIT, "cores": os.cpu_count(),
+                       "kind": "reference",
+                       "sample": f"{len(sb)} blocks ({args.ref_fraction:.3g} class-proportional sample "
+                                 f"of the batch, {pts} interior points), one pass, {secs:.2f} s"}
+        except Exception as ex:  # the baseline is informational; never fail the bench on it
+            cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+                   "sample": f"failed: {ex}"}
+
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": round(val_mixed, 3), "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_mixed, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64 state+stencils / f32 algebra", "data": "synthetic",
+            "config": {"workload": "two-puncture Brill-Lindquist batch: 3000 blocks, padded 13/21/37/69/135 "
+                                   "(1800/750/300/120/30), KO sigma 0.4, mixed precision",
+                       "blocks": len(blocks), "interior_points_per_gpu": npts,
+                       "l2": "inputs (26.7 GB per state) larger than L2; no flush",
+                       "scale": args.scale},
+            "fp64": {"value": round(val_fp64, 3), "ms_per_step": round(ms_fp64, 3),
+                     "deriv_ms": round(d64, 3), "algebra_ms": round(a64, 3)},
+            "mixed_vs_fp64": {"speedup": round(val_mixed / val_fp64, 3),
+                              "max_rel_err": mixed_max_rel, "bar": MIXED_BAR},
+            "kernels_ms": {"deriv": round(d_ms, 3), "algebra": round(a_ms, 3)},
+            "roofline": {"kernel": "bssn_algebra_kernel<float>", "bound": "fp32",
+                         "achieved": round(alg_tf, 3), "peak": round(peak32, 2), "unit": "TFLOP/s",
+                         "frac": round(alg_tf / peak32, 4), "traffic": None,
+                         "peak_source": "measured FMA-chain microbenchmark (b200bssn_fma_peak)",
+                         "flops_per_point": ALGEBRA_FLOPS_PER_POINT},
+            "roofline_fp64": {"kernel": "bssn_algebra_kernel<double>", "bound": "fp64",
+                              "achieved": round(alg64_tf, 3), "peak": round(peak64, 2), "unit": "TFLOP/s",
+                              "frac": round(alg64_tf / peak64, 4)},
+            "gpu_launches": launches,
+            "clocks": clock_info,
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(out), flush=True)
+    for p in plans.values():
+        p.close()
+    ctx.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -134,6 +134,20 @@ int b200bssn_rhs_plan_device(b200bssn_plan *plan, double *const *rhs_dev,
 int b200bssn_rhs_plan_host(b200bssn_plan *plan, double *const *rhs, const double *const *u,
                            uint64_t n_elems, const b200bssn_params *prm);
 
+/* ---- diagnostics ------------------------------------------------------- */
+
+/* Evaluates the plan once on the context stream with CUDA events around each
+ * launch and returns the summed device milliseconds of the derivative kernels
+ * and of the algebra kernels.  Synchronous. */
+int b200bssn_plan_profile(b200bssn_plan *plan, double *const *rhs_dev,
+                          const double *const *u_dev, const b200bssn_params *prm,
+                          double *ms_deriv, double *ms_algebra);
+
+/* Measured FMA throughput of `device` in TFLOP/s (an FMA counts 2 flops) for
+ * FP64 (precision 0) or FP32 (precision 1): the roofline denominator of the
+ * FP-pipe-bound algebra kernel. */
+int b200bssn_fma_peak(int device, uint32_t precision, double *tflops);
+
 #ifdef __cplusplus
 }
 #endif

@@ -105,6 +105,10 @@ SIGNATURES = [
     ("b200bssn_plan_launches", ctypes.c_uint32, [_P]),
     ("b200bssn_rhs_plan_device", ctypes.c_int, [_P, _P, _P, ctypes.POINTER(Params), _P]),
     ("b200bssn_rhs_plan_host", ctypes.c_int, [_P, _P, _P, ctypes.c_uint64, ctypes.POINTER(Params)]),
+    ("b200bssn_plan_profile", ctypes.c_int, [_P, _P, _P, ctypes.POINTER(Params),
+                                             ctypes.POINTER(ctypes.c_double),
+                                             ctypes.POINTER(ctypes.c_double)]),
+    ("b200bssn_fma_peak", ctypes.c_int, [ctypes.c_int, ctypes.c_uint32, ctypes.POINTER(ctypes.c_double)]),
 ]
 
 
@@ -150,6 +154,13 @@ def _ptr_table(arrays: Sequence) -> ctypes.Array:
                 raise ValueError("variable tensors must be contiguous float64")
             ptrs.append(a.data_ptr())
     return (ctypes.c_void_p * NUM_VARS)(*ptrs)
+
+
+def fma_peak_tflops(device: int, precision: int) -> float:
+    """Measured FMA throughput (TFLOP/s) of the device's FP64 or FP32 pipe."""
+    t = ctypes.c_double()
+    _check(load().b200bssn_fma_peak(device, precision, ctypes.byref(t)), "b200bssn_fma_peak")
+    return t.value
 
 
 class Context:
@@ -223,6 +234,14 @@ class Plan:
         _check(load().b200bssn_rhs_plan_device(self.handle, _ptr_table(rhs), _ptr_table(u),
                                                ctypes.byref(params), ctypes.c_void_p(stream or None)),
                "b200bssn_rhs_plan_device", self.ctx)
+
+    def profile(self, rhs, u, params: Params):
+        """One evaluation with per-launch events: (derivative ms, algebra ms)."""
+        d, a = ctypes.c_double(), ctypes.c_double()
+        _check(load().b200bssn_plan_profile(self.handle, _ptr_table(rhs), _ptr_table(u),
+                                            ctypes.byref(params), ctypes.byref(d), ctypes.byref(a)),
+               "b200bssn_plan_profile", self.ctx)
+        return d.value, a.value
 
     def rhs_host(self, rhs, u, n_elems: int, params: Params):
         """Batched RHS on host arrays (H2D, evaluate, D2H; blocks until done)."""

@@ -79,8 +79,10 @@ bool params_ok(const b200bssn_params* p) {
          (p->ghost_policy == B200BSSN_GHOSTS_PRESERVE || p->ghost_policy == B200BSSN_GHOSTS_ZERO);
 }
 
+// Enqueues the plan's launches on `s`.  With `ev` non-null, records an event
+// before and after every launch (ev[4c+0..3] around chunk c's two kernels).
 int launch_plan(b200bssn_plan* P, double* const* rhs, const double* const* u,
-                const b200bssn_params* prm, cudaStream_t s) {
+                const b200bssn_params* prm, cudaStream_t s, cudaEvent_t* ev = nullptr) {
   b200bssn_ctx* ctx = P->ctx;
   DerivArgs da;
   AlgebraArgs aa;
@@ -107,20 +109,25 @@ int launch_plan(b200bssn_plan* P, double* const* rhs, const double* const* u,
   aa.eta_damping_exp = prm->eta_damping_exp;
   aa.ko_sigma = prm->ko_sigma;
   const bool mixed = P->precision == B200BSSN_MIXED;
-  for (const ChunkRec& c : P->chunks) {
+  for (size_t ci = 0; ci < P->chunks.size(); ++ci) {
+    const ChunkRec& c = P->chunks[ci];
     da.tile_base = c.tile_begin;
     aa.range_base = c.range_begin;
     dim3 g1(c.tile_count, kNumVars);
+    if (ev) CK(ctx, cudaEventRecord(ev[4 * ci + 0], s));
     if (mixed)
       bssn_derivs_kernel<float><<<g1, kDerivThreads, kDerivSmemBytes, s>>>(da);
     else
       bssn_derivs_kernel<double><<<g1, kDerivThreads, kDerivSmemBytes, s>>>(da);
     CK(ctx, cudaGetLastError());
+    if (ev) CK(ctx, cudaEventRecord(ev[4 * ci + 1], s));
+    if (ev) CK(ctx, cudaEventRecord(ev[4 * ci + 2], s));
     if (mixed)
       bssn_algebra_kernel<float, float><<<c.range_count, kAlgebraThreads, 0, s>>>(aa);
     else
       bssn_algebra_kernel<double, double><<<c.range_count, kAlgebraThreads, 0, s>>>(aa);
     CK(ctx, cudaGetLastError());
+    if (ev) CK(ctx, cudaEventRecord(ev[4 * ci + 3], s));
   }
   return B200BSSN_OK;
 }
@@ -364,6 +371,34 @@ int b200bssn_rhs_plan_device(b200bssn_plan* P, double* const* rhs_dev, const dou
     if (!rhs_dev[v] || !u_dev[v]) return B200BSSN_ERR_INVALID_ARGUMENT;
   cudaStream_t s = stream ? (cudaStream_t)stream : P->ctx->stream;
   return launch_plan(P, rhs_dev, u_dev, prm, s);
+}
+
+int b200bssn_plan_profile(b200bssn_plan* P, double* const* rhs_dev, const double* const* u_dev,
+                          const b200bssn_params* prm, double* ms_deriv, double* ms_algebra) {
+  if (!P || !rhs_dev || !u_dev || !params_ok(prm) || !ms_deriv || !ms_algebra)
+    return B200BSSN_ERR_INVALID_ARGUMENT;
+  if (prm->precision != P->precision) return B200BSSN_ERR_INVALID_ARGUMENT;
+  b200bssn_ctx* ctx = P->ctx;
+  CK(ctx, cudaSetDevice(ctx->device));
+  std::vector<cudaEvent_t> ev(4 * P->chunks.size());
+  for (auto& e : ev) CK(ctx, cudaEventCreate(&e));
+  int rc = launch_plan(P, rhs_dev, u_dev, prm, ctx->stream, ev.data());
+  if (rc == B200BSSN_OK) {
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) rc = fail_cuda(ctx, e, "profile sync");
+  }
+  double d = 0, a = 0;
+  for (size_t c = 0; rc == B200BSSN_OK && c < P->chunks.size(); ++c) {
+    float t1 = 0, t2 = 0;
+    cudaEventElapsedTime(&t1, ev[4 * c + 0], ev[4 * c + 1]);
+    cudaEventElapsedTime(&t2, ev[4 * c + 2], ev[4 * c + 3]);
+    d += t1;
+    a += t2;
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  *ms_deriv = d;
+  *ms_algebra = a;
+  return rc;
 }
 
 int b200bssn_rhs_plan_host(b200bssn_plan* P, double* const* rhs, const double* const* u,

@@ -1,0 +1,124 @@
+"""CPU tests of the oracle: the C restatement against the reference's own outputs
+(golden fixtures made by tests/golden/make_golden.py from the reference build) and,
+where the reference build is present, against the reference directly."""
+import glob
+import hashlib
+import os
+
+import numpy as np
+import pytest
+
+from oracle import pyoracle as po
+from sympygr_b200 import workloads as wl
+
+TOL = 1e-12  # norm-wise relative, per variable
+
+
+def _sha(u):
+    return hashlib.sha256(np.ascontiguousarray(u, dtype=np.float64).tobytes()).hexdigest()
+
+
+def _fake_cases(golden_dir):
+    return sorted(glob.glob(os.path.join(golden_dir, "fake_*.npz")))
+
+
+def test_golden_files_present(golden_dir):
+    assert len(_fake_cases(golden_dir)) >= 4
+    for name in ("sines_38.npz", "bl_134.npz"):
+        assert os.path.exists(os.path.join(golden_dir, name))
+
+
+@pytest.mark.parametrize("case", ["fake_13_b00", "fake_13_b3f", "fake_13_b05", "fake_17_b2a"])
+def test_oracle_matches_reference_golden_fake(golden_dir, oracle_lib, case):
+    g = np.load(os.path.join(golden_dir, case + ".npz"))
+    u, blk = po.fake_block(int(g["n"]), tuple(g["pmin"]), float(g["h"]), int(g["bflag"]))
+    assert _sha(u) == str(g["input_sha"]), "fake_initial_data restatement drifted"
+    r = po.oracle_rhs(u, blk, po.params(ko_sigma=float(g["sigma"])))
+    mx, rms = po.rel_errors(po.interior(r, blk), g["rhs_interior"])
+    assert mx.max() < TOL, (mx.max(), int(np.argmax(mx)))
+
+
+@pytest.mark.parametrize("name,maker", [("sines_38", lambda: wl.flat_sines(38, 0.1, 0))])
+def test_oracle_matches_reference_golden_cfg1(golden_dir, oracle_lib, name, maker):
+    g = np.load(os.path.join(golden_dir, name + ".npz"))
+    u, blk = maker()
+    assert _sha(u) == str(g["input_sha"])
+    r = po.interior(po.oracle_rhs(u, blk, po.params(ko_sigma=float(g["sigma"]))), blk)
+    ref = g["sample_rhs"]
+    got = r[:, g["sample_index"]]
+    scale = np.abs(g["checksums"][:, 2])[:, None]
+    assert (np.abs(got - ref) / scale).max() < TOL
+    cs = g["checksums"]
+    assert np.allclose(np.abs(r).max(axis=1), cs[:, 2], rtol=1e-12, atol=0)
+    assert np.allclose((r ** 2).sum(axis=1), cs[:, 1], rtol=1e-10, atol=0)
+
+
+def test_workload_inputs_stable(golden_dir):
+    g = np.load(os.path.join(golden_dir, "bl_134.npz"))
+    u, blk = wl.brill_lindquist(134, 8.0, 1.0)
+    assert _sha(u) == str(g["input_sha"])
+    assert blk.bflag == int(g["bflag"]) == 0x3F
+
+
+@pytest.mark.skipif(not po.have_reference("parity"), reason="reference build not present")
+@pytest.mark.parametrize("n,bflag", [(13, 0), (13, 0x3F), (15, 0x11), (21, 0x22), (16, 0x0C)])
+def test_oracle_vs_reference_direct(oracle_lib, n, bflag):
+    u, blk = po.fake_block(n, (-0.4, 0.25, -0.15), 0.06, bflag)
+    prm = po.params(ko_sigma=0.3, eta_r0=0.2, eta_damping_exp=2.0)  # exercise eta damping
+    a = po.oracle_rhs(u, blk, prm)
+    b = po.ref_rhs(u, blk, prm)
+    mx, _ = po.rel_errors(po.interior(a, blk), po.interior(b, blk))
+    assert mx.max() < TOL
+    # ghost points of the RHS are untouched by both
+    mask = ~wl.interior_mask(blk).ravel()
+    assert np.all(a[:, mask] == 0) and np.all(b[:, mask] == 0)
+
+
+def test_ghost_insensitive_with_all_faces(oracle_lib):
+    """With every face flagged, one-sided closures never read the ghost layer."""
+    u, blk = po.fake_block(15, (-0.4, 0.25, -0.15), 0.06, 0x3F)
+    a = po.interior(po.oracle_rhs(u, blk, po.params(ko_sigma=0.2)), blk)
+    u2 = u.copy()
+    mask = ~wl.interior_mask(blk).ravel()
+    u2[:, mask] += np.random.default_rng(3).normal(size=(24, mask.sum()))
+    b = po.interior(po.oracle_rhs(u2, blk, po.params(ko_sigma=0.2)), blk)
+    assert np.array_equal(a, b)
+
+
+def _poly_block(n, deg, axis, bflag):
+    blk = wl.Block(0, (n, n, n), bflag, (-1.0, -0.5, -0.75), (-1.0 + (n - 1) * 0.1,
+                   -0.5 + (n - 1) * 0.1, -0.75 + (n - 1) * 0.1))
+    x, y, z = wl.coords(blk)
+    c = (x, y, z)[axis]
+    return blk, c, c ** deg
+
+
+@pytest.mark.parametrize("axis", [0, 1, 2])
+def test_stencils_exact_on_polynomials(oracle_lib, axis):
+    """Centred first/second derivatives are exact for degree <= 6 polynomials, the
+    4th-order closures for degree <= 4; KO annihilates degree <= 5."""
+    import ctypes
+
+    lib = oracle_lib
+    n = 17
+    fns = {0: ("bssn_oracle_deriv64_x", "bssn_oracle_deriv64_xx", "bssn_oracle_ko_deriv42_x"),
+           1: ("bssn_oracle_deriv64_y", "bssn_oracle_deriv64_yy", "bssn_oracle_ko_deriv42_y"),
+           2: ("bssn_oracle_deriv64_z", "bssn_oracle_deriv64_zz", "bssn_oracle_ko_deriv42_z")}[axis]
+    for bflag, deg in [(0, 6), (0x3F, 4)]:
+        blk, c, f = _poly_block(n, deg, axis, bflag)
+        f = np.ascontiguousarray(f.ravel())
+        sz = (ctypes.c_uint * 3)(n, n, n)
+        inner = wl.interior_mask(blk).ravel()
+        for name, expect, tol in [(fns[0], deg * c.ravel() ** (deg - 1), 1e-8),
+                                  (fns[1], deg * (deg - 1) * c.ravel() ** (deg - 2), 1e-6)]:
+            out = np.zeros_like(f)
+            getattr(lib, name)(out.ctypes.data_as(ctypes.c_void_p), f.ctypes.data_as(ctypes.c_void_p),
+                               ctypes.c_double(0.1), sz, ctypes.c_uint(bflag))
+            err = np.abs(out[inner] - expect[inner]).max() / np.abs(expect[inner]).max()
+            assert err < tol, (name, bflag, err)
+        blk, c, f = _poly_block(n, 5, axis, 0)
+        f = np.ascontiguousarray(f.ravel())
+        out = np.zeros_like(f)
+        getattr(lib, fns[2])(out.ctypes.data_as(ctypes.c_void_p), f.ctypes.data_as(ctypes.c_void_p),
+                             ctypes.c_double(0.1), sz, ctypes.c_uint(0))
+        assert np.abs(out[inner]).max() < 1e-9

@@ -143,6 +143,11 @@ int b200bssn_plan_profile(b200bssn_plan *plan, double *const *rhs_dev,
                           const double *const *u_dev, const b200bssn_params *prm,
                           double *ms_deriv, double *ms_algebra);
 
+/* Copies the derivative scratch of the most recent b200bssn_rhs call on `ctx`
+ * (one block, one chunk) to host `slots` [162][npts]: 138 derivatives, then 24 KO
+ * sums, interior points x fastest.  For checking the stencil stage alone. */
+int b200bssn_debug_block_scratch(b200bssn_ctx *ctx, double *slots, uint64_t npts);
+
 /* Measured FMA throughput of `device` in TFLOP/s (an FMA counts 2 flops) for
  * FP64 (precision 0) or FP32 (precision 1): the roofline denominator of the
  * FP-pipe-bound algebra kernel. */

@@ -108,6 +108,7 @@ SIGNATURES = [
     ("b200bssn_plan_profile", ctypes.c_int, [_P, _P, _P, ctypes.POINTER(Params),
                                              ctypes.POINTER(ctypes.c_double),
                                              ctypes.POINTER(ctypes.c_double)]),
+    ("b200bssn_debug_block_scratch", ctypes.c_int, [_P, _P, ctypes.c_uint64]),
     ("b200bssn_fma_peak", ctypes.c_int, [ctypes.c_int, ctypes.c_uint32, ctypes.POINTER(ctypes.c_double)]),
 ]
 
@@ -197,6 +198,14 @@ class Context:
         s = (ctypes.c_uint32 * 3)(*sz)
         _check(lib.b200bssn_rhs(self.handle, _ptr_table(rhs), _ptr_table(u), int(offset), pm, px,
                                 s, int(bflag), ctypes.byref(params)), "b200bssn_rhs", self)
+
+
+    def debug_block_scratch(self, npts: int) -> np.ndarray:
+        """Derivative slots [162, npts] of the last single-block call."""
+        out = np.zeros((162, npts))
+        _check(load().b200bssn_debug_block_scratch(self.handle, out.ctypes.data_as(ctypes.c_void_p),
+                                                   npts), "b200bssn_debug_block_scratch", self)
+        return out
 
 
 class Plan:

@@ -519,4 +519,28 @@ int b200bssn_rhs(b200bssn_ctx* ctx, double* const* rhs, const double* const* u, 
   return B200BSSN_OK;
 }
 
+int b200bssn_debug_block_scratch(b200bssn_ctx* ctx, double* slots, uint64_t npts) {
+  if (!ctx || !slots || !ctx->blk_plan) return B200BSSN_ERR_INVALID_ARGUMENT;
+  b200bssn_plan* P = ctx->blk_plan;
+  if (P->chunks.size() != 1 || npts != P->points) return B200BSSN_ERR_INVALID_ARGUMENT;
+  CK(ctx, cudaSetDevice(ctx->device));
+  CK(ctx, cudaStreamSynchronize(ctx->stream));
+  std::vector<float> tmp;
+  for (int s = 0; s < kNumDerivs; ++s) {
+    if (P->precision == B200BSSN_MIXED) {
+      tmp.resize(npts);
+      CK(ctx, cudaMemcpy(tmp.data(), static_cast<float*>(P->dscr) + (size_t)s * P->cap,
+                         npts * sizeof(float), cudaMemcpyDeviceToHost));
+      for (uint64_t p = 0; p < npts; ++p) slots[s * npts + p] = tmp[p];
+    } else {
+      CK(ctx, cudaMemcpy(slots + s * npts, static_cast<double*>(P->dscr) + (size_t)s * P->cap,
+                         npts * sizeof(double), cudaMemcpyDeviceToHost));
+    }
+  }
+  for (int v = 0; v < kNumVars; ++v)
+    CK(ctx, cudaMemcpy(slots + (kNumDerivs + v) * npts, P->koscr + (size_t)v * P->cap,
+                       npts * sizeof(double), cudaMemcpyDeviceToHost));
+  return B200BSSN_OK;
+}
+
 }  // extern "C"

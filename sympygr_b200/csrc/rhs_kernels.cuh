@@ -126,9 +126,9 @@ bssn_derivs_kernel(const __grid_constant__ DerivArgs a) {
     }
     const double d2 = line_d1(pu, kSX * kSY, gk, nz, loz, hiz, cz);
     // rhs.cpp:332-369 adds grad_0 + grad_1 + grad_2 of the KO pass in this order
-    const double ko = line_ko(pu, 1, gi, nx, lox, hix, cx) +
-                      line_ko(pu, kSX, gj, ny, loy, hiy, cy) +
-                      line_ko(pu, kSX * kSY, gk, nz, loz, hiz, cz);
+    const double ko = __dadd_rn(__dadd_rn(line_ko(pu, 1, gi, nx, lox, hix, cx),
+                                          line_ko(pu, kSX, gj, ny, loy, hiy, cy)),
+                                line_ko(pu, kSX * kSY, gk, nz, loz, hiz, cz));
     dscr[(3 * v + 0) * cap + lp] = (ST)d0;
     dscr[(3 * v + 1) * cap + lp] = (ST)d1;
     dscr[(3 * v + 2) * cap + lp] = (ST)d2;
@@ -184,7 +184,8 @@ struct PointSink {
   int64_t pp, lp;
   template <typename RT>
   __device__ __forceinline__ void put(int v, RT val) {
-    a->rhs[v][pp] = (double)val + a->ko_sigma * __ldg(a->koscr + v * a->cap + lp);
+    // rhs += sigma * (ko_x + ko_y + ko_z), rounded as rhs.cpp:332-369 rounds it
+    a->rhs[v][pp] = __dadd_rn((double)val, __dmul_rn(a->ko_sigma, __ldg(a->koscr + v * a->cap + lp)));
   }
 };
 
@@ -202,9 +203,11 @@ bssn_algebra_kernel(const __grid_constant__ AlgebraArgs a) {
   const int i = lx + 3, j = ly + 3, k = lz + 3 + un.k0;
   const int64_t pp = B.offset + i + (int64_t)nx * (j + (int64_t)ny * k);
   const int64_t lp = un.sbase + lpu;
-  const double x = B.pmin[0] + i * B.h[0];
-  const double y = B.pmin[1] + j * B.h[1];
-  const double z = B.pmin[2] + k * B.h[2];
+  // coordinates as bssnrhs forms them (pmin + i*h, two roundings, rhs.cpp:207-213)
+  const double x = __dadd_rn(B.pmin[0], __dmul_rn((double)i, B.h[0]));
+  const double y = __dadd_rn(B.pmin[1], __dmul_rn((double)j, B.h[1]));
+  const double z = __dadd_rn(B.pmin[2], __dmul_rn((double)k, B.h[2]));
+  const double r2 = __dadd_rn(__dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y)), __dmul_rn(z, z));
   const uint32_t bf = B.bflag;
   const bool on_face = ((bf & 1u) && i == 3) || ((bf & 2u) && i == nx - 4) ||
                        ((bf & 4u) && j == 3) || ((bf & 8u) && j == ny - 4) ||
@@ -212,7 +215,7 @@ bssn_algebra_kernel(const __grid_constant__ AlgebraArgs a) {
   if (on_face) {
     // bssn_bcs (rhs.cpp:833-977) replaces the algebra on face planes; KO is added
     // afterwards (rhs.cpp:323-369).
-    const double inv_r = 1.0 / sqrt(x * x + y * y + z * z);
+    const double inv_r = 1.0 / sqrt(r2);
     const ST* ds = static_cast<const ST*>(a.dscr);
 #pragma unroll 1
     for (int v = 0; v < kNumVars; ++v) {
@@ -220,14 +223,17 @@ bssn_algebra_kernel(const __grid_constant__ AlgebraArgs a) {
       const double dxf = (double)__ldg(ds + (3 * v + 0) * a.cap + lp);
       const double dyf = (double)__ldg(ds + (3 * v + 1) * a.cap + lp);
       const double dzf = (double)__ldg(ds + (3 * v + 2) * a.cap + lp);
-      const double val =
-          -inv_r * (x * dxf + y * dyf + z * dzf + bc_falloff(v) * (f - bc_asymptotic(v)));
-      a.rhs[v][pp] = val + a.ko_sigma * __ldg(a.koscr + v * a.cap + lp);
+      double t = __dmul_rn(x, dxf);
+      t = __dadd_rn(t, __dmul_rn(y, dyf));
+      t = __dadd_rn(t, __dmul_rn(z, dzf));
+      t = __dadd_rn(t, __dmul_rn(bc_falloff(v), __dsub_rn(f, bc_asymptotic(v))));
+      const double val = __dmul_rn(-inv_r, t);
+      a.rhs[v][pp] = __dadd_rn(val, __dmul_rn(a.ko_sigma, __ldg(a.koscr + v * a.cap + lp)));
     }
     return;
   }
   // eta damping, rhs.cpp:213-219
-  const double r_coord = sqrt(x * x + y * y + z * z);
+  const double r_coord = sqrt(r2);
   double eta = a.eta_const;
   if (r_coord >= a.eta_r0) eta *= pow(a.eta_r0 / r_coord, a.eta_damping_exp);
 

@@ -1,19 +1,26 @@
 // Finite-difference line operators of the reference's default build, evaluated on
 // values staged in shared memory.
 //
-//   d1  : deriv64_{x,y,z}   bssn/src/derivs.cpp:2055-2434  6th-order centred first
-//                                                          derivative, 4th-order closures
-//   d2  : deriv64_{xx,yy,zz} bssn/src/derivs.cpp:2443-2833 6th-order centred second
-//                                                          derivative, 4th-order closures
-//   ko  : ko_deriv42_{x,y,z} bssn/src/derivs.cpp:915-1319  Kreiss-Oliger operator
+//   line_d1 : deriv64_{x,y,z}    bssn/src/derivs.cpp:2055-2434  6th-order centred first
+//                                                               derivative, 4th-order closures
+//   line_d2 : deriv64_{xx,yy,zz} bssn/src/derivs.cpp:2443-2833  6th-order centred second
+//                                                               derivative, 4th-order closures
+//   line_ko : ko_deriv42_{x,y,z} bssn/src/derivs.cpp:915-1319   Kreiss-Oliger operator
 //
 // Each takes a pointer `p` to the value at the evaluation point, the element stride
 // `s` along the operator axis, the point's padded index `pos` on that axis, the
 // padded extent `n`, and whether the low/high face of that axis is a domain
 // boundary (bflag bits).  Closure rows replace the centred row within three points
 // of a flagged face; the high side wins where both apply, as the reference runs
-// its LEFT loop before its RIGHT loop.  Terms are summed in the reference's order.
-// Closure rows reach up to four points inward; callers stage a 4-point halo.
+// its LEFT loop before its RIGHT loop.  Closure rows reach up to four points
+// inward; callers stage a 4-point halo.
+//
+// Rounding: every product and sum is an explicitly rounded IEEE operation
+// (__dmul_rn/__dadd_rn, never contracted into an FMA) taken in the reference's
+// left-to-right order, so each stencil value equals the reference's bit for bit.
+// The stencils cancel terms of size 10^2 |u| down to h|u'|; with contraction the
+// last bits of a first derivative move, and composing two closure rows on a block
+// edge (D_y of D_x) amplifies that to ~1e-12 of the field's range.
 #pragma once
 
 namespace b200bssn {
@@ -40,31 +47,72 @@ __host__ __device__ inline LineScales make_line_scales(double h) {
   return c;
 }
 
-#define B2_AT(k) p[(k) * s]
+// acc + c*v with both operations rounded separately
+__device__ __forceinline__ double mad_rn(double acc, double c, double v) {
+  return __dadd_rn(acc, __dmul_rn(c, v));
+}
+
+// Sum of coefficient[k] * value(offset[k]) in the given order (first term c0*v0).
+#define B2_T(c, k) __dmul_rn((c), p[(k) * s])
+#define B2_Q(c, k) __dmul_rn((c), q[(k) * s])
 
 __device__ __forceinline__ double line_d1(const double* p, int s, int pos, int n, bool lo,
                                           bool hi, const LineScales& c) {
   if (hi && pos >= n - 6) {
     const int r = pos - (n - 6);
-    // q = value at index n-4 (ie-1); rows of derivs.cpp:2132-2155
-    const double* q = p + (n - 4 - pos) * s;
-#define Q(k) q[(k) * s]
-    if (r == 0) return (1.0 * Q(-4) - 8.0 * Q(-3) + 8.0 * Q(-1) - 1.0 * Q(0)) * c.d1_b;
-    if (r == 1) return (-1.0 * Q(-4) + 6.0 * Q(-3) - 18.0 * Q(-2) + 10.0 * Q(-1) + 3.0 * Q(0)) * c.d1_b;
-    return (3.0 * Q(-4) - 16.0 * Q(-3) + 36.0 * Q(-2) - 48.0 * Q(-1) + 25.0 * Q(0)) * c.d1_b;
-#undef Q
+    const double* q = p + (n - 4 - pos) * s;  // value at ie-1 = n-4; derivs.cpp:2132-2155
+    double a;
+    if (r == 0) {
+      a = B2_Q(1.0, -4);
+      a = __dadd_rn(a, B2_Q(-8.0, -3));
+      a = __dadd_rn(a, B2_Q(8.0, -1));
+      a = __dadd_rn(a, B2_Q(-1.0, 0));
+    } else if (r == 1) {
+      a = B2_Q(-1.0, -4);
+      a = __dadd_rn(a, B2_Q(6.0, -3));
+      a = __dadd_rn(a, B2_Q(-18.0, -2));
+      a = __dadd_rn(a, B2_Q(10.0, -1));
+      a = __dadd_rn(a, B2_Q(3.0, 0));
+    } else {
+      a = B2_Q(3.0, -4);
+      a = __dadd_rn(a, B2_Q(-16.0, -3));
+      a = __dadd_rn(a, B2_Q(36.0, -2));
+      a = __dadd_rn(a, B2_Q(-48.0, -1));
+      a = __dadd_rn(a, B2_Q(25.0, 0));
+    }
+    return __dmul_rn(a, c.d1_b);
   }
   if (lo && pos < 6) {
     const int r = pos - 3;
-    const double* q = p - r * s;  // value at index 3; rows of derivs.cpp:2094-2115
-#define Q(k) q[(k) * s]
-    if (r == 0) return (-25.0 * Q(0) + 48.0 * Q(1) - 36.0 * Q(2) + 16.0 * Q(3) - 3.0 * Q(4)) * c.d1_b;
-    if (r == 1) return (-3.0 * Q(0) - 10.0 * Q(1) + 18.0 * Q(2) - 6.0 * Q(3) + 1.0 * Q(4)) * c.d1_b;
-    return (1.0 * Q(0) - 8.0 * Q(1) + 8.0 * Q(3) - 1.0 * Q(4)) * c.d1_b;
-#undef Q
+    const double* q = p - r * s;  // value at index 3; derivs.cpp:2094-2115
+    double a;
+    if (r == 0) {
+      a = B2_Q(-25.0, 0);
+      a = __dadd_rn(a, B2_Q(48.0, 1));
+      a = __dadd_rn(a, B2_Q(-36.0, 2));
+      a = __dadd_rn(a, B2_Q(16.0, 3));
+      a = __dadd_rn(a, B2_Q(-3.0, 4));
+    } else if (r == 1) {
+      a = B2_Q(-3.0, 0);
+      a = __dadd_rn(a, B2_Q(-10.0, 1));
+      a = __dadd_rn(a, B2_Q(18.0, 2));
+      a = __dadd_rn(a, B2_Q(-6.0, 3));
+      a = __dadd_rn(a, B2_Q(1.0, 4));
+    } else {
+      a = B2_Q(1.0, 0);
+      a = __dadd_rn(a, B2_Q(-8.0, 1));
+      a = __dadd_rn(a, B2_Q(8.0, 3));
+      a = __dadd_rn(a, B2_Q(-1.0, 4));
+    }
+    return __dmul_rn(a, c.d1_b);
   }
-  return (-1.0 * B2_AT(-3) + 9.0 * B2_AT(-2) - 45.0 * B2_AT(-1) + 45.0 * B2_AT(1) -
-          9.0 * B2_AT(2) + 1.0 * B2_AT(3)) * c.d1_c;
+  double a = B2_T(-1.0, -3);
+  a = __dadd_rn(a, B2_T(9.0, -2));
+  a = __dadd_rn(a, B2_T(-45.0, -1));
+  a = __dadd_rn(a, B2_T(45.0, 1));
+  a = __dadd_rn(a, B2_T(-9.0, 2));
+  a = __dadd_rn(a, B2_T(1.0, 3));
+  return __dmul_rn(a, c.d1_c);
 }
 
 __device__ __forceinline__ double line_d2(const double* p, int s, int pos, int n, bool lo,
@@ -72,23 +120,61 @@ __device__ __forceinline__ double line_d2(const double* p, int s, int pos, int n
   if (hi && pos >= n - 6) {
     const int r = pos - (n - 6);
     const double* q = p + (n - 4 - pos) * s;  // derivs.cpp:2530-2551
-#define Q(k) q[(k) * s]
-    if (r == 0) return (-1.0 * Q(-4) + 16.0 * Q(-3) - 30.0 * Q(-2) + 16.0 * Q(-1) - 1.0 * Q(0)) * c.d2_b;
-    if (r == 1) return (-1.0 * Q(-4) + 4.0 * Q(-3) + 6.0 * Q(-2) - 20.0 * Q(-1) + 11.0 * Q(0)) * c.d2_b;
-    return (11.0 * Q(-4) - 56.0 * Q(-3) + 114.0 * Q(-2) - 104.0 * Q(-1) + 35.0 * Q(0)) * c.d2_b;
-#undef Q
+    double a;
+    if (r == 0) {
+      a = B2_Q(-1.0, -4);
+      a = __dadd_rn(a, B2_Q(16.0, -3));
+      a = __dadd_rn(a, B2_Q(-30.0, -2));
+      a = __dadd_rn(a, B2_Q(16.0, -1));
+      a = __dadd_rn(a, B2_Q(-1.0, 0));
+    } else if (r == 1) {
+      a = B2_Q(-1.0, -4);
+      a = __dadd_rn(a, B2_Q(4.0, -3));
+      a = __dadd_rn(a, B2_Q(6.0, -2));
+      a = __dadd_rn(a, B2_Q(-20.0, -1));
+      a = __dadd_rn(a, B2_Q(11.0, 0));
+    } else {
+      a = B2_Q(11.0, -4);
+      a = __dadd_rn(a, B2_Q(-56.0, -3));
+      a = __dadd_rn(a, B2_Q(114.0, -2));
+      a = __dadd_rn(a, B2_Q(-104.0, -1));
+      a = __dadd_rn(a, B2_Q(35.0, 0));
+    }
+    return __dmul_rn(a, c.d2_b);
   }
   if (lo && pos < 6) {
     const int r = pos - 3;
     const double* q = p - r * s;  // derivs.cpp:2490-2510
-#define Q(k) q[(k) * s]
-    if (r == 0) return (35.0 * Q(0) - 104.0 * Q(1) + 114.0 * Q(2) - 56.0 * Q(3) + 11.0 * Q(4)) * c.d2_b;
-    if (r == 1) return (11.0 * Q(0) - 20.0 * Q(1) + 6.0 * Q(2) + 4.0 * Q(3) - 1.0 * Q(4)) * c.d2_b;
-    return (-1.0 * Q(0) + 16.0 * Q(1) - 30.0 * Q(2) + 16.0 * Q(3) - 1.0 * Q(4)) * c.d2_b;
-#undef Q
+    double a;
+    if (r == 0) {
+      a = B2_Q(35.0, 0);
+      a = __dadd_rn(a, B2_Q(-104.0, 1));
+      a = __dadd_rn(a, B2_Q(114.0, 2));
+      a = __dadd_rn(a, B2_Q(-56.0, 3));
+      a = __dadd_rn(a, B2_Q(11.0, 4));
+    } else if (r == 1) {
+      a = B2_Q(11.0, 0);
+      a = __dadd_rn(a, B2_Q(-20.0, 1));
+      a = __dadd_rn(a, B2_Q(6.0, 2));
+      a = __dadd_rn(a, B2_Q(4.0, 3));
+      a = __dadd_rn(a, B2_Q(-1.0, 4));
+    } else {
+      a = B2_Q(-1.0, 0);
+      a = __dadd_rn(a, B2_Q(16.0, 1));
+      a = __dadd_rn(a, B2_Q(-30.0, 2));
+      a = __dadd_rn(a, B2_Q(16.0, 3));
+      a = __dadd_rn(a, B2_Q(-1.0, 4));
+    }
+    return __dmul_rn(a, c.d2_b);
   }
-  return (2.0 * B2_AT(-3) - 27.0 * B2_AT(-2) + 270.0 * B2_AT(-1) - 490.0 * B2_AT(0) +
-          270.0 * B2_AT(1) - 27.0 * B2_AT(2) + 2.0 * B2_AT(3)) * c.d2_c;
+  double a = B2_T(2.0, -3);
+  a = __dadd_rn(a, B2_T(-27.0, -2));
+  a = __dadd_rn(a, B2_T(270.0, -1));
+  a = __dadd_rn(a, B2_T(-490.0, 0));
+  a = __dadd_rn(a, B2_T(270.0, 1));
+  a = __dadd_rn(a, B2_T(-27.0, 2));
+  a = __dadd_rn(a, B2_T(2.0, 3));
+  return __dmul_rn(a, c.d2_c);
 }
 
 __device__ __forceinline__ double line_ko(const double* p, int s, int pos, int n, bool lo,
@@ -96,25 +182,66 @@ __device__ __forceinline__ double line_ko(const double* p, int s, int pos, int n
   if (hi && pos >= n - 6) {
     const int r = pos - (n - 6);
     const double* q = p + (n - 4 - pos) * s;  // derivs.cpp:1006-1028
-#define Q(k) q[(k) * s]
-    if (r == 0) return (Q(-5) - 6.0 * Q(-4) + 15.0 * Q(-3) - 19.0 * Q(-2) + 12.0 * Q(-1) - 3.0 * Q(0)) / c.ko_s1;
-    if (r == 1) return (Q(-4) - 6.0 * Q(-3) + 12.0 * Q(-2) - 10.0 * Q(-1) + 3.0 * Q(0)) / c.ko_s2;
-    return (Q(-3) - 3.0 * Q(-2) + 3.0 * Q(-1) - Q(0)) / c.ko_s3;
-#undef Q
+    double a;
+    if (r == 0) {
+      a = q[-5 * s];
+      a = __dadd_rn(a, B2_Q(-6.0, -4));
+      a = __dadd_rn(a, B2_Q(15.0, -3));
+      a = __dadd_rn(a, B2_Q(-19.0, -2));
+      a = __dadd_rn(a, B2_Q(12.0, -1));
+      a = __dadd_rn(a, B2_Q(-3.0, 0));
+      return __ddiv_rn(a, c.ko_s1);
+    } else if (r == 1) {
+      a = q[-4 * s];
+      a = __dadd_rn(a, B2_Q(-6.0, -3));
+      a = __dadd_rn(a, B2_Q(12.0, -2));
+      a = __dadd_rn(a, B2_Q(-10.0, -1));
+      a = __dadd_rn(a, B2_Q(3.0, 0));
+      return __ddiv_rn(a, c.ko_s2);
+    }
+    a = q[-3 * s];
+    a = __dadd_rn(a, B2_Q(-3.0, -2));
+    a = __dadd_rn(a, B2_Q(3.0, -1));
+    a = __dsub_rn(a, q[0]);
+    return __ddiv_rn(a, c.ko_s3);
   }
   if (lo && pos < 6) {
     const int r = pos - 3;
-    const double* q = p - r * s;  // derivs.cpp:969-990
-#define Q(k) q[(k) * s]
-    if (r == 0) return (Q(3) - 3.0 * Q(2) + 3.0 * Q(1) - Q(0)) / c.ko_s3;
-    if (r == 1) return (Q(4) - 6.0 * Q(3) + 12.0 * Q(2) - 10.0 * Q(1) + 3.0 * Q(0)) / c.ko_s2;
-    return (Q(5) - 6.0 * Q(4) + 15.0 * Q(3) - 19.0 * Q(2) + 12.0 * Q(1) - 3.0 * Q(0)) / c.ko_s1;
-#undef Q
+    const double* q = p - r * s;  // derivs.cpp:969-990 (summed from the far point inwards)
+    double a;
+    if (r == 0) {
+      a = q[3 * s];
+      a = __dadd_rn(a, B2_Q(-3.0, 2));
+      a = __dadd_rn(a, B2_Q(3.0, 1));
+      a = __dsub_rn(a, q[0]);
+      return __ddiv_rn(a, c.ko_s3);
+    } else if (r == 1) {
+      a = q[4 * s];
+      a = __dadd_rn(a, B2_Q(-6.0, 3));
+      a = __dadd_rn(a, B2_Q(12.0, 2));
+      a = __dadd_rn(a, B2_Q(-10.0, 1));
+      a = __dadd_rn(a, B2_Q(3.0, 0));
+      return __ddiv_rn(a, c.ko_s2);
+    }
+    a = q[5 * s];
+    a = __dadd_rn(a, B2_Q(-6.0, 4));
+    a = __dadd_rn(a, B2_Q(15.0, 3));
+    a = __dadd_rn(a, B2_Q(-19.0, 2));
+    a = __dadd_rn(a, B2_Q(12.0, 1));
+    a = __dadd_rn(a, B2_Q(-3.0, 0));
+    return __ddiv_rn(a, c.ko_s1);
   }
-  return c.ko_c * (-B2_AT(-3) + 6.0 * B2_AT(-2) - 15.0 * B2_AT(-1) + 20.0 * B2_AT(0) -
-                   15.0 * B2_AT(1) + 6.0 * B2_AT(2) - B2_AT(3));
+  double a = -p[-3 * s];
+  a = __dadd_rn(a, B2_T(6.0, -2));
+  a = __dadd_rn(a, B2_T(-15.0, -1));
+  a = __dadd_rn(a, B2_T(20.0, 0));
+  a = __dadd_rn(a, B2_T(-15.0, 1));
+  a = __dadd_rn(a, B2_T(6.0, 2));
+  a = __dsub_rn(a, p[3 * s]);
+  return __dmul_rn(c.ko_c, a);
 }
 
-#undef B2_AT
+#undef B2_T
+#undef B2_Q
 
 }  // namespace b200bssn

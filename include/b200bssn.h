@@ -134,6 +134,30 @@ int b200bssn_rhs_plan_device(b200bssn_plan *plan, double *const *rhs_dev,
 int b200bssn_rhs_plan_host(b200bssn_plan *plan, double *const *rhs, const double *const *u,
                            uint64_t n_elems, const b200bssn_params *prm);
 
+/* ---- allocation-free variant --------------------------------------------- */
+
+/* Largest interior point count b200bssn_rhs_noalloc accepts: 32^3 (a 38^3
+ * padded block).  Its fixed device array is 42.6 MB. */
+#define B200BSSN_NOALLOC_MAX_POINTS 32768
+
+/* The right-hand side of ONE block on DEVICE arrays without allocating any device
+ * memory.  This entry point has no counterpart in the reference; it exists for
+ * callers that cannot call cudaMalloc: frameworks whose pool allocator owns all of
+ * the GPU's memory, and time-step loops that must avoid the device-wide
+ * synchronisation cudaMalloc/cudaFree can cause.  The caller passes the inputs and
+ * outputs (rhs_dev[v], u_dev[v]: device pointers, block at block->offset) and the
+ * current device is used.  The derivative scratch and the work descriptors live in
+ * one fixed device array inside the library (held by every GPU that loads it until
+ * exit); blocks with more than B200BSSN_NOALLOC_MAX_POINTS interior points are
+ * refused with B200BSSN_ERR_SIZE_LIMIT.  All calls share that array: calls that
+ * overlap on the GPU race and corrupt each other, so serialise them per device.
+ * The first call on a device looks up the array's address (cudaGetSymbolAddress)
+ * and sets a kernel attribute with that device current; make it before any stream
+ * capture.  Asynchronous on `stream` (NULL: the legacy default stream). */
+int b200bssn_rhs_noalloc(double *const *rhs_dev, const double *const *u_dev,
+                         const b200bssn_block *block, const b200bssn_params *prm,
+                         void *stream);
+
 /* ---- diagnostics ------------------------------------------------------- */
 
 /* Evaluates the plan once on the context stream with CUDA events around each

@@ -17,7 +17,7 @@ CSRC = os.path.join(PKG, "csrc")
 LIBDIR = os.path.join(PKG, "lib")
 LIB = os.path.join(LIBDIR, "libb200bssn.so")
 
-SOURCES = ["b200bssn.cu", "diagnostics.cu"]
+SOURCES = ["b200bssn.cu", "diagnostics.cu", "noalloc.cu"]
 HEADERS = ["rhs_kernels.cuh", "stencils.cuh", "plan_types.h", "generated/bssn_rhs_algebra.cuh"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

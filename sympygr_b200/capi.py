@@ -108,6 +108,7 @@ SIGNATURES = [
     ("b200bssn_plan_profile", ctypes.c_int, [_P, _P, _P, ctypes.POINTER(Params),
                                              ctypes.POINTER(ctypes.c_double),
                                              ctypes.POINTER(ctypes.c_double)]),
+    ("b200bssn_rhs_noalloc", ctypes.c_int, [_P, _P, ctypes.POINTER(BlockC), ctypes.POINTER(Params), _P]),
     ("b200bssn_debug_block_scratch", ctypes.c_int, [_P, _P, ctypes.c_uint64]),
     ("b200bssn_fma_peak", ctypes.c_int, [ctypes.c_int, ctypes.c_uint32, ctypes.POINTER(ctypes.c_double)]),
 ]
@@ -155,6 +156,29 @@ def _ptr_table(arrays: Sequence) -> ctypes.Array:
                 raise ValueError("variable tensors must be contiguous float64")
             ptrs.append(a.data_ptr())
     return (ctypes.c_void_p * NUM_VARS)(*ptrs)
+
+
+NOALLOC_MAX_POINTS = 32768
+
+
+def block_struct(b: Block) -> BlockC:
+    c = BlockC()
+    c.offset = b.offset
+    for a in range(3):
+        c.sz[a] = b.sz[a]
+        c.pmin[a] = b.pmin[a]
+        c.pmax[a] = b.pmax[a]
+    c.bflag = b.bflag
+    return c
+
+
+def rhs_noalloc(rhs, u, block: Block, params: Params, stream: int = 0):
+    """One block on device arrays through the allocation-free entry point
+    (b200bssn_rhs_noalloc); asynchronous on `stream` on the current device."""
+    blk = block_struct(block)
+    _check(load().b200bssn_rhs_noalloc(_ptr_table(rhs), _ptr_table(u), ctypes.byref(blk),
+                                       ctypes.byref(params), ctypes.c_void_p(stream or None)),
+           "b200bssn_rhs_noalloc")
 
 
 def fma_peak_tflops(device: int, precision: int) -> float:

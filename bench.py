@@ -149,6 +149,12 @@ def compact_host_batch(blocks):
     return u, out
 
 
+def ref_fraction(args):
+    if args.ref_fraction > 0:
+        return min(1.0, args.ref_fraction)
+    return max(0.1, min(1.0, (os.cpu_count() or 1) / 30.0))
+
+
 def reference_arm(args, rank, world):
     """`--impl reference`: the reference's CPU bssnrhs on this host's cores."""
     if rank != 0:
@@ -160,7 +166,8 @@ def reference_arm(args, rank, world):
         return {"impl": "reference", "unavailable": "reference build oracle/_ref/libbssn_ref_fast.so missing"}
     ncores = os.cpu_count() or 1
     blocks, _ = wl.batch_blocks(seed=0)
-    sample = stratified_blocks(blocks, args.ref_fraction)
+    frac = ref_fraction(args)
+    sample = stratified_blocks(blocks, frac)
     u, sblocks = compact_host_batch(sample)
     # big blocks first so the block-parallel loop does not end on a long tail
     order = sorted(range(len(sblocks)), key=lambda i: -sblocks[i].npad)
@@ -173,8 +180,8 @@ def reference_arm(args, rank, world):
         times.append(s)
     t = statistics.median(times)
     val = pts / t / 1e6
-    sample_desc = (f"{len(sblocks)} of 3000 blocks ({args.ref_fraction:.3g} class-proportional "
-                   f"sample, {pts} interior points) per step; median of {len(times)} steps")
+    sample_desc = (f"{len(sblocks)} of 3000 blocks ({frac:.3g} class-proportional sample, "
+                   f"{pts} interior points, largest blocks first) per step; median of {len(times)} steps")
     return {
         "metric": METRIC, "value": round(val, 4), "unit": UNIT, "impl": "reference",
         "n_gpus": world, "steps": len(times), "warmup": min(args.warmup, 1),
@@ -199,7 +206,9 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--ref-fraction", type=float, default=0.1)
+    ap.add_argument("--ref-fraction", type=float, default=0.0,
+                    help="class-proportional block sample for the CPU reference; 0 = enough "
+                         "135^3 blocks to give every host core one (min 0.1)")
     ap.add_argument("--chunk-points", type=int, default=0)
     args = ap.parse_args()
 
@@ -305,11 +314,12 @@ def main():
     e2e = None
     if not args.no_e2e:
         span = max(b.offset + b.npad for b in blocks)
-        u_h = u.to("cpu").pin_memory() if True else None
+        u_h = torch.empty(tuple(u.shape), dtype=u.dtype, pin_memory=True)
+        u_h.copy_(u)
         del rhs, u
         U = R = None
         torch.cuda.empty_cache()
-        r_h = torch.empty_like(u_h).pin_memory()
+        r_h = torch.empty(tuple(u_h.shape), dtype=u_h.dtype, pin_memory=True)
         p_host = sg.Params.make(ko_sigma=SIGMA, precision=sg.MIXED, ghost_policy=sg.GHOSTS_ZERO)
         UH, RH = [t.data_ptr() for t in u_h], [t.data_ptr() for t in r_h]
         plans[sg.MIXED].rhs_host(RH, UH, span, p_host)  # warm-up (allocates staging)
@@ -326,6 +336,7 @@ def main():
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             ms = t.item()
         nbytes = 24 * span * 8
+        del u_h, r_h
         e2e = {"value": round(total_pts / (ms * 1e-3) / 1e6, 3), "unit": UNIT,
                "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
                "ms_per_step": round(ms, 2), "steps": args.e2e_steps,
@@ -337,14 +348,16 @@ def main():
             from oracle import pyoracle as po
 
             if po.have_reference("fast"):
-                sample = stratified_blocks(blocks, args.ref_fraction)
+                frac = ref_fraction(args)
+                sample = stratified_blocks(blocks, frac)
                 uh, sb = compact_host_batch(sample)
                 sb = [sb[i] for i in sorted(range(len(sb)), key=lambda i: -sb[i].npad)]
                 secs, pts = cpu_reference_run(uh, sb, os.cpu_count() or 1)
+                del uh
                 cpu = {"value": round(pts / secs / 1e6, 4), "unit": UNIT, "cores": os.cpu_count(),
                        "kind": "reference",
-                       "sample": f"{len(sb)} blocks ({args.ref_fraction:.3g} class-proportional sample "
-                                 f"of the batch, {pts} interior points), one pass, {secs:.2f} s"}
+                       "sample": f"{len(sb)} blocks ({frac:.3g} class-proportional sample of the batch, "
+                                 f"{pts} interior points, largest first), one pass, {secs:.2f} s"}
         except Exception as ex:  # the baseline is informational; never fail the bench on it
             cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
                    "sample": f"failed: {ex}"}

@@ -16,6 +16,8 @@ using namespace b200bssn;
 struct b200bssn_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
+  // derivative and algebra streams of the chunk pipeline (see launch_plan)
+  cudaStream_t s_deriv = nullptr, s_alg = nullptr;
   std::string last_error;
   // single-block drop-in path
   double* blk_u = nullptr;    // [24][npad]
@@ -49,8 +51,12 @@ struct b200bssn_plan {
   UnitDev* d_units = nullptr;
   TileDev* d_tiles = nullptr;
   RangeDev* d_ranges = nullptr;
-  void* dscr = nullptr;
-  double* koscr = nullptr;
+  // derivative scratch: two buffers when the plan has more than one chunk, so the
+  // derivative kernel of chunk c+1 can run while the algebra kernel of chunk c reads
+  void* dscr[2] = {nullptr, nullptr};
+  double* koscr[2] = {nullptr, nullptr};
+  std::vector<cudaEvent_t> ev_deriv, ev_alg;  // per chunk: derivative / algebra done
+  cudaEvent_t ev_fork = nullptr;
   // host-batch staging (allocated on first host call)
   double* st_u = nullptr;
   double* st_rhs = nullptr;
@@ -72,15 +78,25 @@ int fail_cuda(b200bssn_ctx* ctx, cudaError_t e, const char* what) {
     if (e_ != cudaSuccess) return fail_cuda(ctx, e_, #call); \
   } while (0)
 
-constexpr int64_t kDefaultChunkPoints = int64_t(1) << 21;
+constexpr int64_t kDefaultChunkPoints = int64_t(1) << 23;
+// scratch slots are addressed with 32-bit offsets: kNumDerivs * cap < 2^31
+constexpr int64_t kMaxChunkPoints = (int64_t(1) << 31) / (kNumDerivs + 1) - 1;
 
 bool params_ok(const b200bssn_params* p) {
   return p && (p->precision == B200BSSN_FP64 || p->precision == B200BSSN_MIXED) &&
          (p->ghost_policy == B200BSSN_GHOSTS_PRESERVE || p->ghost_policy == B200BSSN_GHOSTS_ZERO);
 }
 
-// Enqueues the plan's launches on `s`.  With `ev` non-null, records an event
-// before and after every launch (ev[4c+0..3] around chunk c's two kernels).
+// Enqueues one evaluation of the plan.
+//
+// With `ev` null and more than one chunk the chunks are pipelined over two
+// internal streams: the derivative kernel of chunk c (stream s_deriv, scratch
+// buffer c%2) runs while the algebra kernel of chunk c-1 (stream s_alg) is still
+// reading the other buffer; event edges keep the order K1(c) -> K2(c) and
+// K2(c-2) -> K1(c), and the caller's stream `s` forks into and joins from the
+// two streams, so the whole evaluation is ordered on `s` (and can be captured
+// into a CUDA graph from `s`).  With `ev` non-null (profiling) everything runs on
+// `s` in order, with events ev[4c+0..3] around chunk c's two kernels.
 int launch_plan(b200bssn_plan* P, double* const* rhs, const double* const* u,
                 const b200bssn_params* prm, cudaStream_t s, cudaEvent_t* ev = nullptr) {
   b200bssn_ctx* ctx = P->ctx;
@@ -95,11 +111,7 @@ int launch_plan(b200bssn_plan* P, double* const* rhs, const double* const* u,
   da.units = aa.units = P->d_units;
   da.tiles = P->d_tiles;
   aa.ranges = P->d_ranges;
-  da.dscr = P->dscr;
-  aa.dscr = P->dscr;
-  da.koscr = P->koscr;
-  aa.koscr = P->koscr;
-  da.cap = aa.cap = P->cap;
+  da.cap = aa.cap = (int32_t)P->cap;
   aa.prm64 = {(double)prm->lambda[0], (double)prm->lambda[1], (double)prm->lambda[2],
               (double)prm->lambda[3], prm->lambda_f[0], prm->lambda_f[1]};
   aa.prm32 = {(float)prm->lambda[0], (float)prm->lambda[1], (float)prm->lambda[2],
@@ -109,26 +121,46 @@ int launch_plan(b200bssn_plan* P, double* const* rhs, const double* const* u,
   aa.eta_damping_exp = prm->eta_damping_exp;
   aa.ko_sigma = prm->ko_sigma;
   const bool mixed = P->precision == B200BSSN_MIXED;
-  for (size_t ci = 0; ci < P->chunks.size(); ++ci) {
+  const size_t nch = P->chunks.size();
+  const bool pipelined = ev == nullptr && nch > 1;
+  cudaStream_t s1 = pipelined ? ctx->s_deriv : s, s2 = pipelined ? ctx->s_alg : s;
+  if (pipelined) {
+    CK(ctx, cudaEventRecord(P->ev_fork, s));
+    CK(ctx, cudaStreamWaitEvent(s1, P->ev_fork, 0));
+    CK(ctx, cudaStreamWaitEvent(s2, P->ev_fork, 0));
+  }
+  for (size_t ci = 0; ci < nch; ++ci) {
     const ChunkRec& c = P->chunks[ci];
+    const int buf = pipelined ? (int)(ci & 1) : 0;
     da.tile_base = c.tile_begin;
     aa.range_base = c.range_begin;
-    dim3 g1(c.tile_count, kNumVars);
+    da.dscr = P->dscr[buf];
+    aa.dscr = P->dscr[buf];
+    da.koscr = P->koscr[buf];
+    aa.koscr = P->koscr[buf];
+    if (pipelined && ci >= 2) CK(ctx, cudaStreamWaitEvent(s1, P->ev_alg[ci - 2], 0));
     if (ev) CK(ctx, cudaEventRecord(ev[4 * ci + 0], s));
+    dim3 g1(c.tile_count, 1);
     if (mixed)
-      bssn_derivs_kernel<float><<<g1, kDerivThreads, kDerivSmemBytes, s>>>(da);
+      bssn_derivs_kernel<float><<<g1, kDerivThreads, kDerivSmemBytes, s1>>>(da);
     else
-      bssn_derivs_kernel<double><<<g1, kDerivThreads, kDerivSmemBytes, s>>>(da);
+      bssn_derivs_kernel<double><<<g1, kDerivThreads, kDerivSmemBytes, s1>>>(da);
     CK(ctx, cudaGetLastError());
     if (ev) CK(ctx, cudaEventRecord(ev[4 * ci + 1], s));
+    if (pipelined) {
+      CK(ctx, cudaEventRecord(P->ev_deriv[ci], s1));
+      CK(ctx, cudaStreamWaitEvent(s2, P->ev_deriv[ci], 0));
+    }
     if (ev) CK(ctx, cudaEventRecord(ev[4 * ci + 2], s));
     if (mixed)
-      bssn_algebra_kernel<float, float><<<c.range_count, kAlgebraThreads, 0, s>>>(aa);
+      bssn_algebra_kernel<float, float><<<c.range_count, kAlgebraThreads, 0, s2>>>(aa);
     else
-      bssn_algebra_kernel<double, double><<<c.range_count, kAlgebraThreads, 0, s>>>(aa);
+      bssn_algebra_kernel<double, double><<<c.range_count, kAlgebraThreads, 0, s2>>>(aa);
     CK(ctx, cudaGetLastError());
     if (ev) CK(ctx, cudaEventRecord(ev[4 * ci + 3], s));
+    if (pipelined) CK(ctx, cudaEventRecord(P->ev_alg[ci], s2));
   }
+  if (pipelined) CK(ctx, cudaStreamWaitEvent(s, P->ev_alg[nch - 1], 0));
   return B200BSSN_OK;
 }
 
@@ -191,6 +223,8 @@ int b200bssn_create(b200bssn_ctx** out, int device) {
   int rc = B200BSSN_OK;
   cudaError_t e = cudaSetDevice(device);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->s_deriv, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->s_alg, cudaStreamNonBlocking);
   if (e != cudaSuccess) rc = fail_cuda(ctx, e, "context setup");
   if (rc == B200BSSN_OK) rc = set_kernel_attributes(ctx);
   if (rc != B200BSSN_OK) {
@@ -209,6 +243,8 @@ int b200bssn_destroy(b200bssn_ctx* ctx) {
   cudaFree(ctx->blk_u);
   cudaFree(ctx->blk_rhs);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  if (ctx->s_deriv) cudaStreamDestroy(ctx->s_deriv);
+  if (ctx->s_alg) cudaStreamDestroy(ctx->s_alg);
   delete ctx;
   return B200BSSN_OK;
 }
@@ -261,11 +297,15 @@ int b200bssn_plan_create(b200bssn_ctx* ctx, const b200bssn_block* blocks, uint32
       delete P;
       return B200BSSN_ERR_INVALID_ARGUMENT;
     }
-    for (int64_t k0 = 0; k0 < I2; k0 += kTileZ) {
+    // z-slabs of nearly equal depth (<= kTileZ planes): the derivative kernel
+    // streams each slab plus 4 halo planes on each side
+    const int64_t nslab = (I2 + kTileZ - 1) / kTileZ;
+    for (int64_t sl = 0; sl < nslab; ++sl) {
+      const int64_t k0 = sl * I2 / nslab, k1 = (sl + 1) * I2 / nslab;
       UnitDev u;
       u.block = (int32_t)b;
       u.k0 = (int32_t)k0;
-      u.nz = (int32_t)std::min<int64_t>(kTileZ, I2 - k0);
+      u.nz = (int32_t)(k1 - k0);
       u.pad = 0;
       u.sbase = 0;
       P->units.push_back(u);
@@ -274,7 +314,11 @@ int b200bssn_plan_create(b200bssn_ctx* ctx, const b200bssn_block* blocks, uint32
     P->points += (uint64_t)(I0 * I1 * I2);
   }
   int64_t capacity = chunk_points ? (int64_t)chunk_points : kDefaultChunkPoints;
-  capacity = std::max(capacity, max_unit);
+  capacity = std::min(std::max(capacity, max_unit), kMaxChunkPoints);
+  if (max_unit > kMaxChunkPoints) {
+    delete P;
+    return B200BSSN_ERR_SIZE_LIMIT;
+  }
   // pack units into chunks
   ChunkRec cur{0, 0, 0, 0, 0};
   auto flush = [&]() {
@@ -320,8 +364,18 @@ int b200bssn_plan_create(b200bssn_ctx* ctx, const b200bssn_block* blocks, uint32
   const size_t total = al(nb) + al(nu) + al(nt) + al(nr);
   cudaError_t e = cudaMalloc(&P->desc, total);
   const size_t st = precision == B200BSSN_MIXED ? sizeof(float) : sizeof(double);
-  if (e == cudaSuccess) e = cudaMalloc(&P->dscr, (size_t)kNumDerivs * P->cap * st);
-  if (e == cudaSuccess) e = cudaMalloc((void**)&P->koscr, (size_t)kNumVars * P->cap * sizeof(double));
+  const int nbuf = P->chunks.size() > 1 ? 2 : 1;
+  for (int b = 0; b < nbuf && e == cudaSuccess; ++b) {
+    e = cudaMalloc(&P->dscr[b], (size_t)kNumDerivs * P->cap * st);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&P->koscr[b], (size_t)kNumVars * P->cap * sizeof(double));
+  }
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&P->ev_fork, cudaEventDisableTiming);
+  P->ev_deriv.assign(P->chunks.size(), nullptr);
+  P->ev_alg.assign(P->chunks.size(), nullptr);
+  for (size_t c = 0; c < P->chunks.size() && e == cudaSuccess; ++c) {
+    e = cudaEventCreateWithFlags(&P->ev_deriv[c], cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&P->ev_alg[c], cudaEventDisableTiming);
+  }
   if (e != cudaSuccess) {
     int rc = fail_cuda(ctx, e, "plan allocation");
     b200bssn_plan_destroy(P);
@@ -349,8 +403,19 @@ int b200bssn_plan_destroy(b200bssn_plan* P) {
   if (!P) return B200BSSN_ERR_INVALID_ARGUMENT;
   if (P->ctx) cudaSetDevice(P->ctx->device);
   cudaFree(P->desc);
-  cudaFree(P->dscr);
-  cudaFree(P->koscr);
+  if (P->ctx && P->ctx->stream) {
+    cudaStreamSynchronize(P->ctx->s_deriv);
+    cudaStreamSynchronize(P->ctx->s_alg);
+  }
+  for (int b = 0; b < 2; ++b) {
+    cudaFree(P->dscr[b]);
+    cudaFree(P->koscr[b]);
+  }
+  for (cudaEvent_t e : P->ev_deriv)
+    if (e) cudaEventDestroy(e);
+  for (cudaEvent_t e : P->ev_alg)
+    if (e) cudaEventDestroy(e);
+  if (P->ev_fork) cudaEventDestroy(P->ev_fork);
   cudaFree(P->st_u);
   cudaFree(P->st_rhs);
   delete P;
@@ -529,16 +594,16 @@ int b200bssn_debug_block_scratch(b200bssn_ctx* ctx, double* slots, uint64_t npts
   for (int s = 0; s < kNumDerivs; ++s) {
     if (P->precision == B200BSSN_MIXED) {
       tmp.resize(npts);
-      CK(ctx, cudaMemcpy(tmp.data(), static_cast<float*>(P->dscr) + (size_t)s * P->cap,
+      CK(ctx, cudaMemcpy(tmp.data(), static_cast<float*>(P->dscr[0]) + (size_t)s * P->cap,
                          npts * sizeof(float), cudaMemcpyDeviceToHost));
       for (uint64_t p = 0; p < npts; ++p) slots[s * npts + p] = tmp[p];
     } else {
-      CK(ctx, cudaMemcpy(slots + s * npts, static_cast<double*>(P->dscr) + (size_t)s * P->cap,
+      CK(ctx, cudaMemcpy(slots + s * npts, static_cast<double*>(P->dscr[0]) + (size_t)s * P->cap,
                          npts * sizeof(double), cudaMemcpyDeviceToHost));
     }
   }
   for (int v = 0; v < kNumVars; ++v)
-    CK(ctx, cudaMemcpy(slots + (kNumDerivs + v) * npts, P->koscr + (size_t)v * P->cap,
+    CK(ctx, cudaMemcpy(slots + (kNumDerivs + v) * npts, P->koscr[0] + (size_t)v * P->cap,
                        npts * sizeof(double), cudaMemcpyDeviceToHost));
   return B200BSSN_OK;
 }

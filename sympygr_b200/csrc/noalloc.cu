@@ -184,7 +184,7 @@ extern "C" int b200bssn_rhs_noalloc(double* const* rhs_dev, const double* const*
   aa.dscr = b + kOffDeriv;
   da.koscr = reinterpret_cast<double*>(b + kOffKo);
   aa.koscr = da.koscr;
-  da.cap = aa.cap = kNoallocMaxPoints;
+  da.cap = aa.cap = (int32_t)kNoallocMaxPoints;
   da.tile_base = 0;
   aa.range_base = 0;
   aa.prm64 = {(double)prm->lambda[0], (double)prm->lambda[1], (double)prm->lambda[2],
@@ -196,7 +196,7 @@ extern "C" int b200bssn_rhs_noalloc(double* const* rhs_dev, const double* const*
   aa.eta_damping_exp = prm->eta_damping_exp;
   aa.ko_sigma = prm->ko_sigma;
 
-  const dim3 g1((unsigned)(n_units * tiles_x * tiles_y), kNumVars);
+  const dim3 g1((unsigned)(n_units * tiles_x * tiles_y), 1);
   const unsigned g2 = (unsigned)(n_units * rpu);  // runs past a unit's end have count 0
   if (prm->precision == B200BSSN_MIXED) {
     bssn_derivs_kernel<float><<<g1, kDerivThreads, kDerivSmemBytes, s>>>(da);

@@ -1,13 +1,12 @@
 // The two kernels of one right-hand-side evaluation of a chunk of blocks.
 //
-//  bssn_derivs_kernel   one CTA per (x-y tile of a unit, variable): stages the
-//                       variable's tile with a 4-point halo in shared memory and
-//                       writes, per interior point, the variable's first
-//                       derivatives, its second derivatives when it has them
-//                       (mixed ones as compositions D_y(D_x u), D_z(D_x u),
-//                       D_z(D_y u), exactly as bssn/scripts/bssnrhs_derivs.h
-//                       composes them), and the sum of its three KO terms, into the
-//                       chunk's derivative scratch.
+//  bssn_derivs_kernel   one CTA per 16x16 column tile of a unit, streaming along
+//                       z through every variable: writes, per interior point, the
+//                       variable's first derivatives, its second derivatives when
+//                       it has them (mixed ones as compositions D_y(D_x u),
+//                       D_z(D_x u), D_z(D_y u), exactly as
+//                       bssn/scripts/bssnrhs_derivs.h composes them), and the sum
+//                       of its three KO terms, into the chunk's derivative scratch.
 //  bssn_algebra_kernel  one thread per interior point: the generated BSSN algebra
 //                       (or, on a flagged face plane, the Sommerfeld value of
 //                       bssn/src/rhs.cpp:833-977), plus sigma times the KO sum
@@ -21,9 +20,6 @@
 
 namespace b200bssn {
 
-constexpr int kSX = kTileX + 2 * kHalo, kSY = kTileY + 2 * kHalo, kSZ = kTileZ + 2 * kHalo;
-constexpr int kDerivSmemDoubles = kSZ * kSY * kSX + kSZ * kSY * kTileX + kSZ * kTileY * kTileX;
-constexpr size_t kDerivSmemBytes = sizeof(double) * kDerivSmemDoubles;
 
 // VAR index -> position in the second-derivative list (gt0..gt5, chi, alpha,
 // beta0..2; bssn/scripts/gen_bssnrhs_code:31-32), -1 if none.
@@ -44,106 +40,320 @@ struct DerivArgs {
   const TileDev* tiles;
   void* dscr;        // kNumDerivs slots of `cap` values (double or float)
   double* koscr;     // kNumVars slots of `cap` doubles
-  int64_t cap;
+  int32_t cap;       // kNumDerivs * cap < 2^31: slots use 32-bit offsets
   int32_t tile_base;
 };
 
+// ---------------------------------------------------------------------------
+// Derivative kernel: a 2.5-D streaming stencil.
+//
+// A CTA owns one 16x16 column tile of a unit (a z-slab of up to 48 interior
+// planes of one block) and, for each of the 24 variables in turn, marches along
+// z.  Each z step brings one plane of the tile plus its 4-point x-y halo into
+// shared memory (cp.async, double-buffered: plane z+1 streams in while plane z is
+// differentiated).  In-plane derivatives (D_x, D_y, D_xx, D_yy, D_y(D_x), ko_x,
+// ko_y) come from that plane; the z derivatives of the variable and of its D_x
+// and D_y (D_z, D_zz, ko_z, D_z(D_x), D_z(D_y)) come from 9-deep register queues
+// that each thread keeps for its own column, so every plane is loaded once per
+// variable and no z halo is recomputed.
+// ---------------------------------------------------------------------------
+constexpr int kPlaneW = kTileX + 2 * kHalo;  // 24: plane width incl. halo
+constexpr int kPlaneH = kTileY + 2 * kHalo;  // 24
+constexpr int kPlane = kPlaneW * kPlaneH;     // doubles per staged plane
+constexpr int kDxRows = kTileY + 2 * kHalo;  // D_x rows kept per plane (y halo)
+constexpr int kQ = 2 * kHalo + 1;            // z queue depth (planes z-4 .. z+4)
+static_assert(kTileX == 16 && kTileY == 16 && kDerivThreads == 256, "thread tile is 16x16");
+
+__device__ __forceinline__ void cp_async8(double* smem_dst, const double* gmem_src) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
 template <typename ST>
-__global__ void __launch_bounds__(kDerivThreads)
+__device__ __forceinline__ void put_slot(const DerivArgs& a, int slot, int lp, double val) {
+  static_cast<ST*>(a.dscr)[slot * a.cap + lp] = (ST)val;
+}
+
+// Z-direction rows on a queue q[0..8] holding planes zo-4 .. zo+4 of one column.
+// `zc` selects the row: -1 centred, 0..2 the low-side closure rows (zo = 3,4,5),
+// 3..5 the high-side rows (zo = n-6, n-5, n-4); indices are compile-time in every
+// case, so the queue stays in registers.  Same operations and order as line_*.
+__device__ __forceinline__ int z_case(int zo, int n, bool lo, bool hi) {
+  if (hi && zo >= n - 6) return 3 + (zo - (n - 6));
+  if (lo && zo < 6) return zo - 3;
+  return -1;
+}
+
+#define ZQ(k) q[(k)]
+__device__ __forceinline__ double zq_d1(const double (&q)[kQ], int zc, const LineScales& c) {
+  double a;
+  switch (zc) {
+    case 0:  // zo=3: planes 3..7 -> q[4..8]
+      a = __dmul_rn(-25.0, ZQ(4)); a = mad_rn(a, 48.0, ZQ(5)); a = mad_rn(a, -36.0, ZQ(6));
+      a = mad_rn(a, 16.0, ZQ(7)); a = mad_rn(a, -3.0, ZQ(8));
+      return __dmul_rn(a, c.d1_b);
+    case 1:  // zo=4: planes 3..7 -> q[3..7]
+      a = __dmul_rn(-3.0, ZQ(3)); a = mad_rn(a, -10.0, ZQ(4)); a = mad_rn(a, 18.0, ZQ(5));
+      a = mad_rn(a, -6.0, ZQ(6)); a = mad_rn(a, 1.0, ZQ(7));
+      return __dmul_rn(a, c.d1_b);
+    case 2:  // zo=5: planes 3,4,6,7 -> q[2,3,5,6]
+      a = __dmul_rn(1.0, ZQ(2)); a = mad_rn(a, -8.0, ZQ(3)); a = mad_rn(a, 8.0, ZQ(5));
+      a = mad_rn(a, -1.0, ZQ(6));
+      return __dmul_rn(a, c.d1_b);
+    case 3:  // zo=n-6: planes n-8,n-7,n-5,n-4 -> q[2,3,5,6]
+      a = __dmul_rn(1.0, ZQ(2)); a = mad_rn(a, -8.0, ZQ(3)); a = mad_rn(a, 8.0, ZQ(5));
+      a = mad_rn(a, -1.0, ZQ(6));
+      return __dmul_rn(a, c.d1_b);
+    case 4:  // zo=n-5: planes n-8..n-4 -> q[1..5]
+      a = __dmul_rn(-1.0, ZQ(1)); a = mad_rn(a, 6.0, ZQ(2)); a = mad_rn(a, -18.0, ZQ(3));
+      a = mad_rn(a, 10.0, ZQ(4)); a = mad_rn(a, 3.0, ZQ(5));
+      return __dmul_rn(a, c.d1_b);
+    case 5:  // zo=n-4: planes n-8..n-4 -> q[0..4]
+      a = __dmul_rn(3.0, ZQ(0)); a = mad_rn(a, -16.0, ZQ(1)); a = mad_rn(a, 36.0, ZQ(2));
+      a = mad_rn(a, -48.0, ZQ(3)); a = mad_rn(a, 25.0, ZQ(4));
+      return __dmul_rn(a, c.d1_b);
+    default:
+      return win_d1(q, 4, c);
+  }
+}
+
+__device__ __forceinline__ double zq_d2(const double (&q)[kQ], int zc, const LineScales& c) {
+  double a;
+  switch (zc) {
+    case 0:
+      a = __dmul_rn(35.0, ZQ(4)); a = mad_rn(a, -104.0, ZQ(5)); a = mad_rn(a, 114.0, ZQ(6));
+      a = mad_rn(a, -56.0, ZQ(7)); a = mad_rn(a, 11.0, ZQ(8));
+      return __dmul_rn(a, c.d2_b);
+    case 1:
+      a = __dmul_rn(11.0, ZQ(3)); a = mad_rn(a, -20.0, ZQ(4)); a = mad_rn(a, 6.0, ZQ(5));
+      a = mad_rn(a, 4.0, ZQ(6)); a = mad_rn(a, -1.0, ZQ(7));
+      return __dmul_rn(a, c.d2_b);
+    case 2:
+      a = __dmul_rn(-1.0, ZQ(2)); a = mad_rn(a, 16.0, ZQ(3)); a = mad_rn(a, -30.0, ZQ(4));
+      a = mad_rn(a, 16.0, ZQ(5)); a = mad_rn(a, -1.0, ZQ(6));
+      return __dmul_rn(a, c.d2_b);
+    case 3:
+      a = __dmul_rn(-1.0, ZQ(2)); a = mad_rn(a, 16.0, ZQ(3)); a = mad_rn(a, -30.0, ZQ(4));
+      a = mad_rn(a, 16.0, ZQ(5)); a = mad_rn(a, -1.0, ZQ(6));
+      return __dmul_rn(a, c.d2_b);
+    case 4:
+      a = __dmul_rn(-1.0, ZQ(1)); a = mad_rn(a, 4.0, ZQ(2)); a = mad_rn(a, 6.0, ZQ(3));
+      a = mad_rn(a, -20.0, ZQ(4)); a = mad_rn(a, 11.0, ZQ(5));
+      return __dmul_rn(a, c.d2_b);
+    case 5:
+      a = __dmul_rn(11.0, ZQ(0)); a = mad_rn(a, -56.0, ZQ(1)); a = mad_rn(a, 114.0, ZQ(2));
+      a = mad_rn(a, -104.0, ZQ(3)); a = mad_rn(a, 35.0, ZQ(4));
+      return __dmul_rn(a, c.d2_b);
+    default:
+      return win_d2(q, 4, c);
+  }
+}
+
+__device__ __forceinline__ double zq_ko(const double (&q)[kQ], int zc, const LineScales& c) {
+  double a;
+  switch (zc) {
+    case 0:  // (u6 - 3u5 + 3u4 - u3)/s3, planes 3..6 -> q[4..7]
+      a = ZQ(7); a = mad_rn(a, -3.0, ZQ(6)); a = mad_rn(a, 3.0, ZQ(5)); a = __dsub_rn(a, ZQ(4));
+      return __ddiv_rn(a, c.ko_s3);
+    case 1:  // planes 3..7 -> q[3..7]
+      a = ZQ(7); a = mad_rn(a, -6.0, ZQ(6)); a = mad_rn(a, 12.0, ZQ(5)); a = mad_rn(a, -10.0, ZQ(4));
+      a = mad_rn(a, 3.0, ZQ(3));
+      return __ddiv_rn(a, c.ko_s2);
+    case 2:  // planes 3..8 -> q[2..7]
+      a = ZQ(7); a = mad_rn(a, -6.0, ZQ(6)); a = mad_rn(a, 15.0, ZQ(5)); a = mad_rn(a, -19.0, ZQ(4));
+      a = mad_rn(a, 12.0, ZQ(3)); a = mad_rn(a, -3.0, ZQ(2));
+      return __ddiv_rn(a, c.ko_s1);
+    case 3:  // zo=n-6: planes n-9..n-4 -> q[1..6]
+      a = ZQ(1); a = mad_rn(a, -6.0, ZQ(2)); a = mad_rn(a, 15.0, ZQ(3)); a = mad_rn(a, -19.0, ZQ(4));
+      a = mad_rn(a, 12.0, ZQ(5)); a = mad_rn(a, -3.0, ZQ(6));
+      return __ddiv_rn(a, c.ko_s1);
+    case 4:  // zo=n-5: planes n-9..n-4 -> q[0..5]... rows use n-9+1 .. n-4 -> q[1..5]
+      a = ZQ(1); a = mad_rn(a, -6.0, ZQ(2)); a = mad_rn(a, 12.0, ZQ(3)); a = mad_rn(a, -10.0, ZQ(4));
+      a = mad_rn(a, 3.0, ZQ(5));
+      return __ddiv_rn(a, c.ko_s2);
+    case 5:  // zo=n-4: planes n-7..n-4 -> q[1..4]
+      a = ZQ(1); a = mad_rn(a, -3.0, ZQ(2)); a = mad_rn(a, 3.0, ZQ(3)); a = __dsub_rn(a, ZQ(4));
+      return __ddiv_rn(a, c.ko_s3);
+    default:
+      return win_ko(q, 4, c);
+  }
+}
+#undef ZQ
+
+template <int N>
+__device__ __forceinline__ void q_push(double (&q)[N], double v) {
+#pragma unroll
+  for (int k = 0; k < N - 1; ++k) q[k] = q[k + 1];
+  q[N - 1] = v;
+}
+
+template <typename ST>
+__global__ void __launch_bounds__(kDerivThreads, 2)
 bssn_derivs_kernel(const __grid_constant__ DerivArgs a) {
-  extern __shared__ double smem[];
-  double* s_u = smem;                        // [kSZ][kSY][kSX]
-  double* s_dx = s_u + kSZ * kSY * kSX;      // [kSZ][kSY][kTileX]
-  double* s_dy = s_dx + kSZ * kSY * kTileX;  // [kSZ][kTileY][kTileX]
+  __shared__ double s_plane[2][kPlane];           // staged planes (tile + x-y halo)
+  __shared__ double s_dxp[kDxRows * kTileX];      // D_x of the current plane, y halo rows
+  __shared__ LineScales s_sc[3];
 
   const TileDev t = a.tiles[a.tile_base + blockIdx.x];
   const UnitDev un = a.units[t.unit];
-  const BlockDev B = a.blocks[un.block];
-  const int v = blockIdx.y;
-  const int q = dd_index(v);
+  const BlockDev& B = a.blocks[un.block];
   const int nx = B.sz[0], ny = B.sz[1], nz = B.sz[2];
   const int I0 = nx - 6, I1 = ny - 6;
   const int i0 = 3 + t.i0, j0 = 3 + t.j0, k0 = 3 + un.k0;
   const int ex = t.ex, ey = t.ey, ez = un.nz;
-  const int ox = i0 - kHalo, oy = j0 - kHalo, oz = k0 - kHalo;  // smem origin (padded coords)
+  const int ox = i0 - kHalo, oy = j0 - kHalo;  // plane origin (padded coords)
   const int xlo = max(0, ox), xhi = min(nx, i0 + ex + kHalo);
   const int ylo = max(0, oy), yhi = min(ny, j0 + ey + kHalo);
-  const int zlo = max(0, oz), zhi = min(nz, k0 + ez + kHalo);
-  const int lx = xhi - xlo, ly = yhi - ylo, lz = zhi - zlo;
-
-  const double* __restrict__ f = a.u[v] + B.offset;
-  for (int idx = threadIdx.x; idx < lx * ly * lz; idx += blockDim.x) {
-    const int x = idx % lx, r = idx / lx, y = r % ly, z = r / ly;
-    const int gi = xlo + x, gj = ylo + y, gk = zlo + z;
-    s_u[((gk - oz) * kSY + (gj - oy)) * kSX + (gi - ox)] =
-        __ldg(f + gi + (int64_t)nx * (gj + (int64_t)ny * gk));
-  }
-  __syncthreads();
-
-  const LineScales cx = make_line_scales(B.h[0]);
-  const LineScales cy = make_line_scales(B.h[1]);
-  const LineScales cz = make_line_scales(B.h[2]);
   const uint32_t bf = B.bflag;
   const bool lox = bf & 1u, hix = bf & 2u, loy = bf & 4u, hiy = bf & 8u, loz = bf & 16u,
              hiz = bf & 32u;
+  if (threadIdx.x < 3) s_sc[threadIdx.x] = make_line_scales(B.h[threadIdx.x]);
 
-  if (q >= 0) {
-    // D_x on the tile's x range over the y/z halo (deriv64_x covers all j,k,
-    // bssn/src/derivs.cpp:2067-2068), then D_y on the tile's x-y range over the z
-    // halo (deriv64_y covers all k, :2199-2202).
-    for (int idx = threadIdx.x; idx < ex * ly * lz; idx += blockDim.x) {
-      const int x = idx % ex, r = idx / ex, y = r % ly, z = r / ly;
-      const int gi = i0 + x, gj = ylo + y, gk = zlo + z;
-      const double* pu = &s_u[((gk - oz) * kSY + (gj - oy)) * kSX + (gi - ox)];
-      s_dx[((gk - oz) * kSY + (gj - oy)) * kTileX + x] = line_d1(pu, 1, gi, nx, lox, hix, cx);
-    }
-    for (int idx = threadIdx.x; idx < ex * ey * lz; idx += blockDim.x) {
-      const int x = idx % ex, r = idx / ex, y = r % ey, z = r / ey;
-      const int gi = i0 + x, gj = j0 + y, gk = zlo + z;
-      const double* pu = &s_u[((gk - oz) * kSY + (gj - oy)) * kSX + (gi - ox)];
-      s_dy[((gk - oz) * kTileY + y) * kTileX + x] = line_d1(pu, kSX, gj, ny, loy, hiy, cy);
-    }
-    __syncthreads();
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const bool active = tx < ex && ty < ey;
+  const int gi = i0 + tx, gj = j0 + ty;
+  // chunk-relative scratch offsets fit in 32 bits (kNumDerivs * cap < 2^31)
+  const int plane_pts = I0 * I1;
+  const int lp_col = (int)un.sbase + (gi - 3) + I0 * (gj - 3);  // + plane_pts * (z - k0)
+  const int zs = max(0, k0 - kHalo);
+  const int zend = k0 + ez + kHalo;  // exclusive; planes >= nz are not loaded
+  const bool clx = closure_row(gi, nx, lox, hix), cly = closure_row(gj, ny, loy, hiy);
+
+  // This thread's share of a plane copy (fixed for the whole CTA): column bx of
+  // the 32-wide staging grid, rows by0, by0+8, by0+16 of the 24-row plane.
+  const int sbx = threadIdx.x & 31, sby0 = threadIdx.x >> 5;
+  int st_soff[3], st_goff[3];
+  bool st_ok[3];
+#pragma unroll
+  for (int r = 0; r < 3; ++r) {
+    const int by = sby0 + 8 * r, pi = ox + sbx, pj = oy + by;
+    st_ok[r] = sbx < kPlaneW && pi >= xlo && pi < xhi && pj >= ylo && pj < yhi;
+    st_soff[r] = by * kPlaneW + sbx;
+    st_goff[r] = pi + nx * pj;
   }
+  // and of the y-halo D_x rows: column dxx, rows dyy0 and dyy0 + 16
+  const int dxx = threadIdx.x & 15, dyy0 = threadIdx.x >> 4;
+  const int dpi = i0 + dxx;
+  const bool dcl = closure_row(dpi, nx, lox, hix);
+  bool dx_ok[2];
+#pragma unroll
+  for (int r = 0; r < 2; ++r) {
+    const int yy = dyy0 + 16 * r, pj = oy + yy;
+    dx_ok[r] = yy < kDxRows && dxx < ex && pj >= ylo && pj < yhi;
+  }
+  const int64_t plane_elems = (int64_t)nx * ny;
 
-  ST* __restrict__ dscr = static_cast<ST*>(a.dscr);
-  const int64_t cap = a.cap;
-  for (int idx = threadIdx.x; idx < ex * ey * ez; idx += blockDim.x) {
-    const int x = idx % ex, r = idx / ex, y = r % ey, z = r / ey;
-    const int gi = i0 + x, gj = j0 + y, gk = k0 + z;
-    const double* pu = &s_u[((gk - oz) * kSY + (gj - oy)) * kSX + (gi - ox)];
-    const int64_t lp = un.sbase + (gi - 3) + (int64_t)I0 * ((gj - 3) + (int64_t)I1 * (gk - k0));
+  for (int v = 0; v < kNumVars; ++v) {
+    const int q = dd_index(v);
+    const double* __restrict__ f = a.u[v] + B.offset;
+    double qu[kQ], qx[kQ], qy[kQ], qk[kHalo + 1];
+#pragma unroll
+    for (int k = 0; k < kQ; ++k) qu[k] = qx[k] = qy[k] = 0.0;
+#pragma unroll
+    for (int k = 0; k <= kHalo; ++k) qk[k] = 0.0;
 
-    double d0, d1;
-    const double* pdx = &s_dx[((gk - oz) * kSY + (gj - oy)) * kTileX + x];
-    const double* pdy = &s_dy[((gk - oz) * kTileY + y) * kTileX + x];
-    if (q >= 0) {
-      d0 = *pdx;
-      d1 = *pdy;
-    } else {
-      d0 = line_d1(pu, 1, gi, nx, lox, hix, cx);
-      d1 = line_d1(pu, kSX, gj, ny, loy, hiy, cy);
+    // stage plane zi into buffer b (one commit group; empty when zi >= nz)
+    auto stage = [&](int zi, int b) {
+      if (zi < nz) {
+        const double* fp = f + plane_elems * zi;
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+          if (st_ok[r]) cp_async8(&s_plane[b][st_soff[r]], fp + st_goff[r]);
+      }
+      cp_async_commit();
+    };
+
+    __syncthreads();  // previous variable's readers are done with both buffers
+    stage(zs, 0);
+    for (int zi = zs; zi < zend; ++zi) {
+      const int b = (zi - zs) & 1;
+      stage(zi + 1, b ^ 1);
+      cp_async_wait<1>();
+      __syncthreads();
+      const double* P = s_plane[b];
+      const bool in_block = zi < nz;
+      const bool out_plane = zi >= k0 && zi < k0 + ez;
+
+      // D_x of this plane on the tile's x range and the y halo rows (only the
+      // variables with mixed derivatives need the halo rows).
+      if (q >= 0 && in_block) {
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+          if (dx_ok[r]) {
+            const int yy = dyy0 + 16 * r;
+            const double* p = P + yy * kPlaneW + dxx + kHalo;
+            s_dxp[yy * kTileX + dxx] = dcl ? line_d1_cl(p, 1, dpi, nx, lox, hix, s_sc[0])
+                                           : line_d1(p, 1, dpi, nx, false, false, s_sc[0]);
+          }
+        }
+        __syncthreads();
+      }
+
+      double dx = 0.0, dy = 0.0, kxy = 0.0, u0 = 0.0;
+      if (active && in_block) {
+        const double* pc = P + (ty + kHalo) * kPlaneW + (tx + kHalo);
+        u0 = *pc;
+        double wx[7], wy[7];
+#pragma unroll
+        for (int k = 0; k < 7; ++k) {
+          wx[k] = pc[k - 3];
+          wy[k] = pc[(k - 3) * kPlaneW];
+        }
+        const LineScales& cx = s_sc[0];
+        const LineScales& cy = s_sc[1];
+        dx = q >= 0 ? s_dxp[(ty + kHalo) * kTileX + tx]
+                    : (clx ? line_d1_cl(pc, 1, gi, nx, lox, hix, cx) : win_d1(wx, 3, cx));
+        dy = cly ? line_d1_cl(pc, kPlaneW, gj, ny, loy, hiy, cy) : win_d1(wy, 3, cy);
+        if (out_plane) {
+          const int lp = lp_col + plane_pts * (zi - k0);
+          const double kx = clx ? line_ko_cl(pc, 1, gi, nx, lox, hix, cx) : win_ko(wx, 3, cx);
+          const double ky = cly ? line_ko_cl(pc, kPlaneW, gj, ny, loy, hiy, cy) : win_ko(wy, 3, cy);
+          kxy = __dadd_rn(kx, ky);
+          put_slot<ST>(a, 3 * v + 0, lp, dx);
+          put_slot<ST>(a, 3 * v + 1, lp, dy);
+          if (q >= 0) {
+            const int s0 = 72 + 6 * q;
+            put_slot<ST>(a, s0 + 0, lp, clx ? line_d2_cl(pc, 1, gi, nx, lox, hix, cx) : win_d2(wx, 3, cx));
+            put_slot<ST>(a, s0 + 3, lp, cly ? line_d2_cl(pc, kPlaneW, gj, ny, loy, hiy, cy) : win_d2(wy, 3, cy));
+            const double* pd = s_dxp + (ty + kHalo) * kTileX + tx;
+            double wd[7];
+#pragma unroll
+            for (int k = 0; k < 7; ++k) wd[k] = pd[(k - 3) * kTileX];
+            put_slot<ST>(a, s0 + 1, lp, cly ? line_d1_cl(pd, kTileX, gj, ny, loy, hiy, cy) : win_d1(wd, 3, cy));
+          }
+        }
+      }
+      q_push(qu, u0);
+      q_push(qx, dx);
+      q_push(qy, dy);
+      q_push(qk, kxy);
+
+      // z derivatives of plane zo = zi - 4, whose +-4 neighbourhood is now queued
+      const int zo = zi - kHalo;
+      if (active && zo >= k0 && zo < k0 + ez) {
+        const LineScales& cz = s_sc[2];
+        const int zc = z_case(zo, nz, loz, hiz);
+        const int lp = lp_col + plane_pts * (zo - k0);
+        put_slot<ST>(a, 3 * v + 2, lp, zq_d1(qu, zc, cz));
+        // rhs.cpp:332-369 sums (ko_x + ko_y) + ko_z
+        a.koscr[v * a.cap + lp] = __dadd_rn(qk[0], zq_ko(qu, zc, cz));
+        if (q >= 0) {
+          const int s0 = 72 + 6 * q;
+          put_slot<ST>(a, s0 + 5, lp, zq_d2(qu, zc, cz));
+          put_slot<ST>(a, s0 + 2, lp, zq_d1(qx, zc, cz));
+          put_slot<ST>(a, s0 + 4, lp, zq_d1(qy, zc, cz));
+        }
+      }
+      __syncthreads();  // buffer b and s_dxp are rewritten next step
     }
-    const double d2 = line_d1(pu, kSX * kSY, gk, nz, loz, hiz, cz);
-    // rhs.cpp:332-369 adds grad_0 + grad_1 + grad_2 of the KO pass in this order
-    const double ko = __dadd_rn(__dadd_rn(line_ko(pu, 1, gi, nx, lox, hix, cx),
-                                          line_ko(pu, kSX, gj, ny, loy, hiy, cy)),
-                                line_ko(pu, kSX * kSY, gk, nz, loz, hiz, cz));
-    dscr[(3 * v + 0) * cap + lp] = (ST)d0;
-    dscr[(3 * v + 1) * cap + lp] = (ST)d1;
-    dscr[(3 * v + 2) * cap + lp] = (ST)d2;
-    a.koscr[v * cap + lp] = ko;
-    if (q >= 0) {
-      const int s0 = 72 + 6 * q;
-      dscr[(s0 + 0) * cap + lp] = (ST)line_d2(pu, 1, gi, nx, lox, hix, cx);
-      dscr[(s0 + 1) * cap + lp] = (ST)line_d1(pdx, kTileX, gj, ny, loy, hiy, cy);
-      dscr[(s0 + 2) * cap + lp] = (ST)line_d1(pdx, kSY * kTileX, gk, nz, loz, hiz, cz);
-      dscr[(s0 + 3) * cap + lp] = (ST)line_d2(pu, kSX, gj, ny, loy, hiy, cy);
-      dscr[(s0 + 4) * cap + lp] = (ST)line_d1(pdy, kTileY * kTileX, gk, nz, loz, hiz, cz);
-      dscr[(s0 + 5) * cap + lp] = (ST)line_d2(pu, kSX * kSY, gk, nz, loz, hiz, cz);
-    }
+    cp_async_wait<0>();
   }
 }
+
+constexpr size_t kDerivSmemBytes = 0;  // all shared memory is static
 
 struct AlgebraArgs {
   const double* u[kNumVars];
@@ -153,7 +363,7 @@ struct AlgebraArgs {
   const RangeDev* ranges;
   const void* dscr;
   const double* koscr;
-  int64_t cap;
+  int32_t cap;
   int32_t range_base;
   AlgebraParams<double> prm64;
   AlgebraParams<float> prm32;
@@ -172,7 +382,7 @@ template <typename RT, typename ST>
 struct PointIn {
   const AlgebraArgs* a;
   int64_t pp;   // element index of the point in the variable arrays
-  int64_t lp;   // scratch index
+  int lp;       // scratch index
   __device__ __forceinline__ RT u(int v) const { return (RT)__ldg(a->u[v] + pp); }
   __device__ __forceinline__ RT d(int s) const {
     return (RT)__ldg(static_cast<const ST*>(a->dscr) + s * a->cap + lp);
@@ -181,7 +391,8 @@ struct PointIn {
 
 struct PointSink {
   const AlgebraArgs* a;
-  int64_t pp, lp;
+  int64_t pp;
+  int lp;
   template <typename RT>
   __device__ __forceinline__ void put(int v, RT val) {
     // rhs += sigma * (ko_x + ko_y + ko_z), rounded as rhs.cpp:332-369 rounds it
@@ -202,7 +413,7 @@ bssn_algebra_kernel(const __grid_constant__ AlgebraArgs a) {
   const int lx = lpu % I0, rr = lpu / I0, ly = rr % I1, lz = rr / I1;
   const int i = lx + 3, j = ly + 3, k = lz + 3 + un.k0;
   const int64_t pp = B.offset + i + (int64_t)nx * (j + (int64_t)ny * k);
-  const int64_t lp = un.sbase + lpu;
+  const int lp = (int)un.sbase + lpu;
   // coordinates as bssnrhs forms them (pmin + i*h, two roundings, rhs.cpp:207-213)
   const double x = __dadd_rn(B.pmin[0], __dmul_rn((double)i, B.h[0]));
   const double y = __dadd_rn(B.pmin[1], __dmul_rn((double)j, B.h[1]));

@@ -244,4 +244,66 @@ __device__ __forceinline__ double line_ko(const double* p, int s, int pos, int n
 #undef B2_T
 #undef B2_Q
 
+// Centred rows on a register window w[] (C = index of the evaluation point).
+// Callers invoke these inside fully unrolled loops, so every index folds to a
+// constant and the window stays in registers.  Same operations and order as the
+// centred branches above.
+template <int N>
+__device__ __forceinline__ double win_d1(const double (&w)[N], const int C,
+                                         const LineScales& c) {
+  double a = __dmul_rn(-1.0, w[C - 3]);
+  a = mad_rn(a, 9.0, w[C - 2]);
+  a = mad_rn(a, -45.0, w[C - 1]);
+  a = mad_rn(a, 45.0, w[C + 1]);
+  a = mad_rn(a, -9.0, w[C + 2]);
+  a = mad_rn(a, 1.0, w[C + 3]);
+  return __dmul_rn(a, c.d1_c);
+}
+
+template <int N>
+__device__ __forceinline__ double win_d2(const double (&w)[N], const int C,
+                                         const LineScales& c) {
+  double a = __dmul_rn(2.0, w[C - 3]);
+  a = mad_rn(a, -27.0, w[C - 2]);
+  a = mad_rn(a, 270.0, w[C - 1]);
+  a = mad_rn(a, -490.0, w[C]);
+  a = mad_rn(a, 270.0, w[C + 1]);
+  a = mad_rn(a, -27.0, w[C + 2]);
+  a = mad_rn(a, 2.0, w[C + 3]);
+  return __dmul_rn(a, c.d2_c);
+}
+
+template <int N>
+__device__ __forceinline__ double win_ko(const double (&w)[N], const int C,
+                                         const LineScales& c) {
+  double a = -w[C - 3];
+  a = mad_rn(a, 6.0, w[C - 2]);
+  a = mad_rn(a, -15.0, w[C - 1]);
+  a = mad_rn(a, 20.0, w[C]);
+  a = mad_rn(a, -15.0, w[C + 1]);
+  a = mad_rn(a, 6.0, w[C + 2]);
+  a = __dsub_rn(a, w[C + 3]);
+  return __dmul_rn(c.ko_c, a);
+}
+
+// Out-of-line closure evaluations: only points next to flagged faces take them,
+// so keeping them out of the unrolled window loops keeps those loops small.
+static __device__ __noinline__ double line_d1_cl(const double* p, int s, int pos, int n, bool lo, bool hi,
+                                          const LineScales& c) {
+  return line_d1(p, s, pos, n, lo, hi, c);
+}
+static __device__ __noinline__ double line_d2_cl(const double* p, int s, int pos, int n, bool lo, bool hi,
+                                          const LineScales& c) {
+  return line_d2(p, s, pos, n, lo, hi, c);
+}
+static __device__ __noinline__ double line_ko_cl(const double* p, int s, int pos, int n, bool lo, bool hi,
+                                          const LineScales& c) {
+  return line_ko(p, s, pos, n, lo, hi, c);
+}
+
+// True when the point at padded index `pos` takes a closure row.
+__device__ __forceinline__ bool closure_row(int pos, int n, bool lo, bool hi) {
+  return (lo && pos < 6) || (hi && pos >= n - 6);
+}
+
 }  // namespace b200bssn

@@ -8,8 +8,9 @@ for device code that is instantiated at more than one precision:
 * every numeric constant is printed as a cast to the arithmetic type ``RT``
   (``((RT)0.6666666666666666)``), so the same text compiles to FP64 or FP32
   arithmetic without silent promotion of float expressions to double;
-* integer powers are products as in the parent, negative powers become one
-  division (``((RT)1)/(x*x)``), and ``x**(1/2)`` maps to ``sqrt``;
+* integer powers are parenthesised products (the parent's bare ``x*x`` would
+  print ``y/x**2`` as ``y/x*x``), negative powers become one division
+  (``((RT)1)/((x*x))``), and ``x**(1/2)`` maps to ``sqrt``;
 * symbols print as bare identifiers: the generator binds every input (state
   value, derivative, parameter) to a local of that name.
 
@@ -64,7 +65,9 @@ def make_printers(dendro_c_printer_cls):
             if ex.is_Integer:
                 n = int(ex)
                 if 2 <= n <= 6:
-                    return "*".join([self.parenthesize(base, prec)] * n)
+                    # parenthesised: the product may stand in a denominator,
+                    # where a bare x*x would read as (1/x)*x
+                    return "(%s)" % "*".join([self.parenthesize(base, prec)] * n)
                 if -6 <= n <= -1:
                     return "((%s)1)/(%s)" % (
                         self.rt,

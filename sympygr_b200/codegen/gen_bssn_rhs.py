@@ -92,6 +92,55 @@ def _input_binding(sym_name, slots, flavor):
     raise KeyError(sym_name)
 
 
+def emit_staged(stages, printer, slots):
+    """CUDA body for the staged capture (staged.py): each stage is CSE'd on its own
+    and its values are bound to named locals before the next stage starts; the
+    last stage's outputs go to the sink.  Returns (lines, ops after CSE, temps)."""
+    lines = []
+    seen_inputs = set()
+    nops = ntmp = 0
+    stage_syms = set()
+    for si, (name, defs) in enumerate(stages):
+        syms = [d[0] for d in defs]
+        exprs = [d[1] for d in defs]
+        repl, reduced = sp.cse(exprs, symbols=sp.numbered_symbols(f"s{si}_t"), optimizations="basic")
+        ntmp += len(repl)
+        lines.append("  // ---- stage %s: %d values, %d temporaries" % (name, len(defs), len(repl)))
+        last = name == "out"
+        tmp_index = {t: i for i, (t, _) in enumerate(repl)}
+        ready_after = {}
+        for sym, e in zip(syms, reduced):
+            deps = [tmp_index[x] for x in e.free_symbols if x in tmp_index]
+            ready_after.setdefault(max(deps) if deps else -1, []).append((sym, e))
+
+        def bind(expr):
+            for x in sorted(expr.free_symbols, key=lambda z: z.name):
+                if x in tmp_index or x in seen_inputs or x in stage_syms or x.name == "eta":
+                    continue
+                seen_inputs.add(x)
+                lines.append("  const RT %s = %s;" % (x.name, _input_binding(x.name, slots, "cuda")))
+
+        def put(sym, e):
+            nonlocal nops
+            nops += sp.count_ops(e)
+            bind(e)
+            if last:
+                lines.append("  sink.put(%d, %s);  // %s" % (OUT_VAR[sym], printer.doprint(e), sym))
+            else:
+                lines.append("  const RT %s = %s;" % (sym.name, printer.doprint(e)))
+                stage_syms.add(sym)
+
+        for sym, e in ready_after.get(-1, []):
+            put(sym, e)
+        for i, (t, e) in enumerate(repl):
+            nops += sp.count_ops(e)
+            bind(e)
+            lines.append("  const RT %s = %s;" % (t.name, printer.doprint(e)))
+            for sym, oe in ready_after.get(i, []):
+                put(sym, oe)
+    return lines, nops, ntmp
+
+
 def emit(prog, printer, flavor, slots):
     lines = []
     rt = "RT" if flavor == "cuda" else "double"
@@ -147,6 +196,16 @@ __device__ __forceinline__ void bssn_rhs_algebra(const In& in, Sink& sink,
                                                  const AlgebraParams<RT>& prm, const RT eta) {
 """
 
+CUDA_HEADER_STAGED = CUDA_HEADER.replace(
+    "// expressions of GR/bssn.py:57-105 (bssn_puncture_gauge), CSE'd with\n"
+    "// sympy.cse(optimizations='basic') and printed by CudaPrinter (a subclass of\n"
+    "// dendrosym/code_printer.py:DendroCPrinter).",
+    "// expressions of GR/bssn.py:57-105 (bssn_puncture_gauge), built in stages\n"
+    "// (inverse metric, Christoffels, CalGt, Ricci tensor, outputs; see\n"
+    "// sympygr_b200/codegen/staged.py), each stage CSE'd on its own with\n"
+    "// sympy.cse(optimizations='basic') and printed by CudaPrinter (a subclass of\n"
+    "// dendrosym/code_printer.py:DendroCPrinter).")
+
 C_HEADER = """\
 /* TEST INFRASTRUCTURE ONLY (oracle).
  * GENERATED by sympygr_b200/codegen/gen_bssn_rhs.py -- do not edit by hand.
@@ -176,6 +235,8 @@ def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", required=True, help="root of the SymPyGR checkout")
     ap.add_argument("--cache", default=None, help="optional pickle to reuse the CSE")
+    ap.add_argument("--flat-cuda", action="store_true",
+                    help="print the CUDA algebra from the single global CSE (as the C oracle)")
     args = ap.parse_args(argv)
 
     t0 = time.time()
@@ -195,10 +256,19 @@ def main(argv=None):
     slots = src.derivative_slots()
     prog = schedule(names, repl, reduced)
 
-    body, nops = emit(prog, CudaPrinter(), "cuda", slots)
+    if args.flat_cuda:
+        body, nops = emit(prog, CudaPrinter(), "cuda", slots)
+        ntmp = len(repl)
+        header = CUDA_HEADER
+    else:
+        from .staged import capture_staged
+
+        stages = capture_staged(args.reference)
+        body, nops, ntmp = emit_staged(stages, CudaPrinter(), slots)
+        header = CUDA_HEADER_STAGED
     os.makedirs(os.path.dirname(CUDA_OUT), exist_ok=True)
     with open(CUDA_OUT, "w") as f:
-        f.write(CUDA_HEADER % {"orig": orig, "nops": nops, "ntmp": len(repl)})
+        f.write(header % {"orig": orig, "nops": nops, "ntmp": ntmp})
         f.write("\n".join(body))
         f.write("\n}\n\n}  // namespace b200bssn\n")
 

@@ -1,0 +1,51 @@
+// Host build of the generated device algebra (sympygr_b200/csrc/generated/
+// bssn_rhs_algebra.cuh) next to the oracle's C algebra, at seeded random points.
+// Prints the largest norm-wise relative difference per output over all points.
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <random>
+#define __device__
+#define __forceinline__ inline
+using std::sqrt;
+#include "bssn_rhs_algebra.cuh"
+extern "C" void bssn_oracle_algebra(const double*, const double*, const double*, double, double*);
+struct In {
+  const double* u_;
+  const double* d_;
+  double u(int v) const { return u_[v]; }
+  double d(int s) const { return d_[s]; }
+};
+struct Sink {
+  double* o;
+  void put(int v, double x) { o[v] = x; }
+};
+int main(int argc, char** argv) {
+  const int npts = argc > 1 ? std::atoi(argv[1]) : 2000;
+  std::mt19937_64 g(12345);
+  std::uniform_real_distribution<double> U(-0.3, 0.3);
+  double maxdiff[24] = {0}, maxref[24] = {0};
+  const double par[6] = {1, 1, 1, 1, 1, 0};
+  const b200bssn::AlgebraParams<double> prm{1, 1, 1, 1, 1, 0};
+  for (int t = 0; t < npts; ++t) {
+    double u[24], d[138], a[24], b[24];
+    for (double& x : u) x = U(g);
+    u[0] = 0.8 + U(g);
+    u[1] = 0.8 + U(g);
+    u[12] = 1 + 0.3 * U(g);
+    u[15] = 1 + 0.3 * U(g);
+    u[17] = 1 + 0.3 * U(g);
+    for (double& x : d) x = U(g);
+    const double eta = 2.0 + U(g);
+    In in{u, d};
+    Sink s{a};
+    b200bssn::bssn_rhs_algebra<double>(in, s, prm, eta);
+    bssn_oracle_algebra(u, d, par, eta, b);
+    for (int v = 0; v < 24; ++v) {
+      maxdiff[v] = std::fmax(maxdiff[v], std::fabs(a[v] - b[v]));
+      maxref[v] = std::fmax(maxref[v], std::fabs(b[v]));
+    }
+  }
+  for (int v = 0; v < 24; ++v) std::printf("%d %.6e\n", v, maxdiff[v] / std::fmax(maxref[v], 1e-300));
+  return 0;
+}

@@ -1,0 +1,23 @@
+"""CPU check of the generated device algebra: the staged CUDA template, compiled
+for the host with RT=double, against the oracle's flat C algebra (which is pinned
+to the reference's bssneqs_eta_const_standard_gauge.cpp through the golden tests)
+at seeded random points.  Catches printer and generator mistakes without a GPU."""
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(HERE)
+
+
+def test_staged_device_algebra_matches_oracle(tmp_path):
+    exe = str(tmp_path / "algcheck")
+    subprocess.run(["g++", "-O1", "-std=c++17", os.path.join(HERE, "algebra_host_check.cpp"),
+                    os.path.join(REPO, "oracle", "bssn_oracle_algebra.c"),
+                    "-I", os.path.join(REPO, "sympygr_b200", "csrc", "generated"),
+                    "-I", os.path.join(REPO, "oracle"), "-o", exe, "-lm"], check=True)
+    out = subprocess.run([exe, "3000"], capture_output=True, text=True, check=True).stdout
+    rel = np.array([float(l.split()[1]) for l in out.strip().splitlines()])
+    assert rel.shape == (24,)
+    assert rel.max() < 1e-13, rel

@@ -57,6 +57,8 @@ struct b200bssn_plan {
   double* koscr[2] = {nullptr, nullptr};
   std::vector<cudaEvent_t> ev_deriv, ev_alg;  // per chunk: derivative / algebra done
   cudaEvent_t ev_fork = nullptr;
+  int* d_counters = nullptr;  // per chunk: work counter of the derivative kernel
+  int deriv_grid = 0;         // resident CTAs of the persistent derivative kernel
   // host-batch staging (allocated on first host call)
   double* st_u = nullptr;
   double* st_rhs = nullptr;
@@ -124,6 +126,7 @@ int launch_plan(b200bssn_plan* P, double* const* rhs, const double* const* u,
   const size_t nch = P->chunks.size();
   const bool pipelined = ev == nullptr && nch > 1;
   cudaStream_t s1 = pipelined ? ctx->s_deriv : s, s2 = pipelined ? ctx->s_alg : s;
+  CK(ctx, cudaMemsetAsync(P->d_counters, 0, nch * sizeof(int), s));
   if (pipelined) {
     CK(ctx, cudaEventRecord(P->ev_fork, s));
     CK(ctx, cudaStreamWaitEvent(s1, P->ev_fork, 0));
@@ -140,7 +143,9 @@ int launch_plan(b200bssn_plan* P, double* const* rhs, const double* const* u,
     aa.koscr = P->koscr[buf];
     if (pipelined && ci >= 2) CK(ctx, cudaStreamWaitEvent(s1, P->ev_alg[ci - 2], 0));
     if (ev) CK(ctx, cudaEventRecord(ev[4 * ci + 0], s));
-    dim3 g1(c.tile_count, 1);
+    da.tile_count = c.tile_count;
+    da.counter = P->d_counters + ci;
+    dim3 g1(std::min(c.tile_count * kNumVars, P->deriv_grid), 1);
     if (mixed)
       bssn_derivs_kernel<float><<<g1, kDerivThreads, kDerivSmemBytes, s1>>>(da);
     else
@@ -357,6 +362,25 @@ int b200bssn_plan_create(b200bssn_ctx* ctx, const b200bssn_block* blocks, uint32
     }
   }
   flush();
+  // longest tiles first within each chunk (cost ~ planes streamed)
+  for (const ChunkRec& c : P->chunks) {
+    auto planes = [&](const TileDev& t) {
+      const UnitDev& u = P->units[t.unit];
+      const BlockDev& B = P->blocks[u.block];
+      return std::min(B.sz[2], 3 + u.k0 + u.nz + kHalo) - std::max(0, 3 + u.k0 - kHalo);
+    };
+    std::stable_sort(P->tiles.begin() + c.tile_begin, P->tiles.begin() + c.tile_begin + c.tile_count,
+                     [&](const TileDev& x, const TileDev& y) { return planes(x) > planes(y); });
+  }
+  {
+    int sms = 0, per_sm = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &per_sm, precision == B200BSSN_MIXED ? (const void*)bssn_derivs_kernel<float>
+                                             : (const void*)bssn_derivs_kernel<double>,
+        kDerivThreads, kDerivSmemBytes);
+    P->deriv_grid = std::max(1, sms * std::max(1, per_sm));
+  }
 
   const size_t nb = P->blocks.size() * sizeof(BlockDev), nu = P->units.size() * sizeof(UnitDev),
                nt = P->tiles.size() * sizeof(TileDev), nr = P->ranges.size() * sizeof(RangeDev);
@@ -370,6 +394,7 @@ int b200bssn_plan_create(b200bssn_ctx* ctx, const b200bssn_block* blocks, uint32
     if (e == cudaSuccess) e = cudaMalloc((void**)&P->koscr[b], (size_t)kNumVars * P->cap * sizeof(double));
   }
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&P->ev_fork, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&P->d_counters, P->chunks.size() * sizeof(int));
   P->ev_deriv.assign(P->chunks.size(), nullptr);
   P->ev_alg.assign(P->chunks.size(), nullptr);
   for (size_t c = 0; c < P->chunks.size() && e == cudaSuccess; ++c) {
@@ -416,6 +441,7 @@ int b200bssn_plan_destroy(b200bssn_plan* P) {
   for (cudaEvent_t e : P->ev_alg)
     if (e) cudaEventDestroy(e);
   if (P->ev_fork) cudaEventDestroy(P->ev_fork);
+  cudaFree(P->d_counters);
   cudaFree(P->st_u);
   cudaFree(P->st_rhs);
   delete P;

@@ -41,7 +41,8 @@ constexpr int kMaxDevices = 64;
 
 // byte layout of the fixed array (each part 256-byte aligned)
 constexpr size_t al256(size_t x) { return (x + 255) & ~size_t(255); }
-constexpr size_t kOffBlock = 0;
+constexpr size_t kOffCounter = 0;
+constexpr size_t kOffBlock = kOffCounter + 256;
 constexpr size_t kOffUnits = kOffBlock + al256(sizeof(BlockDev));
 constexpr size_t kOffTiles = kOffUnits + al256(sizeof(UnitDev) * kNoallocMaxUnits);
 constexpr size_t kOffRanges = kOffTiles + al256(sizeof(TileDev) * kNoallocMaxTiles);
@@ -81,10 +82,13 @@ int setup_device(int dev, void** addr) {
 // Writes the work descriptors of one block (z-slab units of kTileZ planes, x-y
 // tiles, runs of kAlgebraThreads points) -- the layout b200bssn_plan_create
 // builds on the host -- straight into the fixed array.
-__global__ void noalloc_describe(BlockDev blk, BlockDev* blk_out, UnitDev* units, TileDev* tiles,
-                                 RangeDev* ranges, int n_units, int tiles_x, int tiles_y,
-                                 int ranges_per_unit_max) {
-  if (blockIdx.x == 0 && threadIdx.x == 0) *blk_out = blk;
+__global__ void noalloc_describe(BlockDev blk, BlockDev* blk_out, int* counter, UnitDev* units,
+                                 TileDev* tiles, RangeDev* ranges, int n_units, int tiles_x,
+                                 int tiles_y, int ranges_per_unit_max) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    *blk_out = blk;
+    *counter = 0;  // work counter of the derivative kernel
+  }
   const int I0 = blk.sz[0] - 6, I1 = blk.sz[1] - 6, I2 = blk.sz[2] - 6;
   const int tiles_per_unit = tiles_x * tiles_y;
   for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < n_units; u += gridDim.x * blockDim.x) {
@@ -165,8 +169,9 @@ extern "C" int b200bssn_rhs_noalloc(double* const* rhs_dev, const double* const*
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   // the block descriptor travels as a kernel argument and the kernel stores it,
   // so no host-to-device copy is needed either
-  noalloc_describe<<<(int)((n_units + 127) / 128), 128, 0, s>>>(blk, bd, units, tiles, ranges,
-                                                                (int)n_units, (int)tiles_x,
+  int* counter = reinterpret_cast<int*>(b + kOffCounter);
+  noalloc_describe<<<(int)((n_units + 127) / 128), 128, 0, s>>>(blk, bd, counter, units, tiles,
+                                                                ranges, (int)n_units, (int)tiles_x,
                                                                 (int)tiles_y, (int)rpu);
 
   DerivArgs da;
@@ -186,6 +191,8 @@ extern "C" int b200bssn_rhs_noalloc(double* const* rhs_dev, const double* const*
   aa.koscr = da.koscr;
   da.cap = aa.cap = (int32_t)kNoallocMaxPoints;
   da.tile_base = 0;
+  da.tile_count = (int32_t)(n_units * tiles_x * tiles_y);
+  da.counter = counter;
   aa.range_base = 0;
   aa.prm64 = {(double)prm->lambda[0], (double)prm->lambda[1], (double)prm->lambda[2],
               (double)prm->lambda[3], prm->lambda_f[0], prm->lambda_f[1]};
@@ -196,7 +203,7 @@ extern "C" int b200bssn_rhs_noalloc(double* const* rhs_dev, const double* const*
   aa.eta_damping_exp = prm->eta_damping_exp;
   aa.ko_sigma = prm->ko_sigma;
 
-  const dim3 g1((unsigned)(n_units * tiles_x * tiles_y), 1);
+  const dim3 g1((unsigned)(n_units * tiles_x * tiles_y * kNumVars), 1);
   const unsigned g2 = (unsigned)(n_units * rpu);  // runs past a unit's end have count 0
   if (prm->precision == B200BSSN_MIXED) {
     bssn_derivs_kernel<float><<<g1, kDerivThreads, kDerivSmemBytes, s>>>(da);

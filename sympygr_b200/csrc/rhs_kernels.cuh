@@ -42,14 +42,15 @@ struct DerivArgs {
   double* koscr;     // kNumVars slots of `cap` doubles
   int32_t cap;       // kNumDerivs * cap < 2^31: slots use 32-bit offsets
   int32_t tile_base;
+  int32_t tile_count;
+  int* counter;      // work counter of this launch, zero at launch
 };
 
 // ---------------------------------------------------------------------------
 // Derivative kernel: a 2.5-D streaming stencil.
 //
-// A CTA owns one 16x16 column tile of a unit (a z-slab of up to 48 interior
-// planes of one block) and, for each of the 24 variables in turn, marches along
-// z.  Each z step brings one plane of the tile plus its 4-point x-y halo into
+// A work item is one 16x16 column tile of a unit (a z-slab of up to 48 interior
+// planes of one block) and one variable; the CTA marches along z.  Each z step brings one plane of the tile plus its 4-point x-y halo into
 // shared memory (cp.async, double-buffered: plane z+1 streams in while plane z is
 // differentiated).  In-plane derivatives (D_x, D_y, D_xx, D_yy, D_y(D_x), ko_x,
 // ko_y) come from that plane; the z derivatives of the variable and of its D_x
@@ -72,87 +73,83 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
-template <typename ST>
-__device__ __forceinline__ void put_slot(const DerivArgs& a, int slot, int lp, double val) {
+template <typename ST, typename V>
+__device__ __forceinline__ void put_slot(const DerivArgs& a, int slot, int lp, V val) {
   static_cast<ST*>(a.dscr)[slot * a.cap + lp] = (ST)val;
 }
 
 // Z-direction rows on a queue q[0..8] holding planes zo-4 .. zo+4 of one column.
 // `zc` selects the row: -1 centred, 0..2 the low-side closure rows (zo = 3,4,5),
 // 3..5 the high-side rows (zo = n-6, n-5, n-4); indices are compile-time in every
-// case, so the queue stays in registers.  Same operations and order as line_*.
+// case, so the queue stays in registers.  Same operations and order as line_*;
+// values are widened to double (exact for double queues).
 __device__ __forceinline__ int z_case(int zo, int n, bool lo, bool hi) {
   if (hi && zo >= n - 6) return 3 + (zo - (n - 6));
   if (lo && zo < 6) return zo - 3;
   return -1;
 }
 
-#define ZQ(k) q[(k)]
-__device__ __forceinline__ double zq_d1(const double (&q)[kQ], int zc, const LineScales& c) {
+#define ZQ(k) ((double)q[(k)])
+template <typename T>
+__device__ __forceinline__ double zq_d1_closure(const T (&q)[kQ], int zc, const LineScales& c) {
   double a;
   switch (zc) {
     case 0:  // zo=3: planes 3..7 -> q[4..8]
       a = __dmul_rn(-25.0, ZQ(4)); a = mad_rn(a, 48.0, ZQ(5)); a = mad_rn(a, -36.0, ZQ(6));
       a = mad_rn(a, 16.0, ZQ(7)); a = mad_rn(a, -3.0, ZQ(8));
-      return __dmul_rn(a, c.d1_b);
+      break;
     case 1:  // zo=4: planes 3..7 -> q[3..7]
       a = __dmul_rn(-3.0, ZQ(3)); a = mad_rn(a, -10.0, ZQ(4)); a = mad_rn(a, 18.0, ZQ(5));
       a = mad_rn(a, -6.0, ZQ(6)); a = mad_rn(a, 1.0, ZQ(7));
-      return __dmul_rn(a, c.d1_b);
+      break;
     case 2:  // zo=5: planes 3,4,6,7 -> q[2,3,5,6]
-      a = __dmul_rn(1.0, ZQ(2)); a = mad_rn(a, -8.0, ZQ(3)); a = mad_rn(a, 8.0, ZQ(5));
-      a = mad_rn(a, -1.0, ZQ(6));
-      return __dmul_rn(a, c.d1_b);
     case 3:  // zo=n-6: planes n-8,n-7,n-5,n-4 -> q[2,3,5,6]
       a = __dmul_rn(1.0, ZQ(2)); a = mad_rn(a, -8.0, ZQ(3)); a = mad_rn(a, 8.0, ZQ(5));
       a = mad_rn(a, -1.0, ZQ(6));
-      return __dmul_rn(a, c.d1_b);
+      break;
     case 4:  // zo=n-5: planes n-8..n-4 -> q[1..5]
       a = __dmul_rn(-1.0, ZQ(1)); a = mad_rn(a, 6.0, ZQ(2)); a = mad_rn(a, -18.0, ZQ(3));
       a = mad_rn(a, 10.0, ZQ(4)); a = mad_rn(a, 3.0, ZQ(5));
-      return __dmul_rn(a, c.d1_b);
-    case 5:  // zo=n-4: planes n-8..n-4 -> q[0..4]
+      break;
+    default:  // 5: zo=n-4: planes n-8..n-4 -> q[0..4]
       a = __dmul_rn(3.0, ZQ(0)); a = mad_rn(a, -16.0, ZQ(1)); a = mad_rn(a, 36.0, ZQ(2));
       a = mad_rn(a, -48.0, ZQ(3)); a = mad_rn(a, 25.0, ZQ(4));
-      return __dmul_rn(a, c.d1_b);
-    default:
-      return win_d1(q, 4, c);
+      break;
   }
+  return __dmul_rn(a, c.d1_b);
 }
 
-__device__ __forceinline__ double zq_d2(const double (&q)[kQ], int zc, const LineScales& c) {
+template <typename T>
+__device__ __forceinline__ double zq_d2_closure(const T (&q)[kQ], int zc, const LineScales& c) {
   double a;
   switch (zc) {
     case 0:
       a = __dmul_rn(35.0, ZQ(4)); a = mad_rn(a, -104.0, ZQ(5)); a = mad_rn(a, 114.0, ZQ(6));
       a = mad_rn(a, -56.0, ZQ(7)); a = mad_rn(a, 11.0, ZQ(8));
-      return __dmul_rn(a, c.d2_b);
+      break;
     case 1:
       a = __dmul_rn(11.0, ZQ(3)); a = mad_rn(a, -20.0, ZQ(4)); a = mad_rn(a, 6.0, ZQ(5));
       a = mad_rn(a, 4.0, ZQ(6)); a = mad_rn(a, -1.0, ZQ(7));
-      return __dmul_rn(a, c.d2_b);
+      break;
     case 2:
-      a = __dmul_rn(-1.0, ZQ(2)); a = mad_rn(a, 16.0, ZQ(3)); a = mad_rn(a, -30.0, ZQ(4));
-      a = mad_rn(a, 16.0, ZQ(5)); a = mad_rn(a, -1.0, ZQ(6));
-      return __dmul_rn(a, c.d2_b);
     case 3:
       a = __dmul_rn(-1.0, ZQ(2)); a = mad_rn(a, 16.0, ZQ(3)); a = mad_rn(a, -30.0, ZQ(4));
       a = mad_rn(a, 16.0, ZQ(5)); a = mad_rn(a, -1.0, ZQ(6));
-      return __dmul_rn(a, c.d2_b);
+      break;
     case 4:
       a = __dmul_rn(-1.0, ZQ(1)); a = mad_rn(a, 4.0, ZQ(2)); a = mad_rn(a, 6.0, ZQ(3));
       a = mad_rn(a, -20.0, ZQ(4)); a = mad_rn(a, 11.0, ZQ(5));
-      return __dmul_rn(a, c.d2_b);
-    case 5:
+      break;
+    default:
       a = __dmul_rn(11.0, ZQ(0)); a = mad_rn(a, -56.0, ZQ(1)); a = mad_rn(a, 114.0, ZQ(2));
       a = mad_rn(a, -104.0, ZQ(3)); a = mad_rn(a, 35.0, ZQ(4));
-      return __dmul_rn(a, c.d2_b);
-    default:
-      return win_d2(q, 4, c);
+      break;
   }
+  return __dmul_rn(a, c.d2_b);
 }
 
-__device__ __forceinline__ double zq_ko(const double (&q)[kQ], int zc, const LineScales& c) {
+template <typename T>
+__device__ __forceinline__ double zq_ko_closure(const T (&q)[kQ], int zc, const LineScales& c) {
   double a;
   switch (zc) {
     case 0:  // (u6 - 3u5 + 3u4 - u3)/s3, planes 3..6 -> q[4..7]
@@ -170,34 +167,142 @@ __device__ __forceinline__ double zq_ko(const double (&q)[kQ], int zc, const Lin
       a = ZQ(1); a = mad_rn(a, -6.0, ZQ(2)); a = mad_rn(a, 15.0, ZQ(3)); a = mad_rn(a, -19.0, ZQ(4));
       a = mad_rn(a, 12.0, ZQ(5)); a = mad_rn(a, -3.0, ZQ(6));
       return __ddiv_rn(a, c.ko_s1);
-    case 4:  // zo=n-5: planes n-9..n-4 -> q[0..5]... rows use n-9+1 .. n-4 -> q[1..5]
+    case 4:  // zo=n-5: planes n-8..n-4 -> q[1..5]
       a = ZQ(1); a = mad_rn(a, -6.0, ZQ(2)); a = mad_rn(a, 12.0, ZQ(3)); a = mad_rn(a, -10.0, ZQ(4));
       a = mad_rn(a, 3.0, ZQ(5));
       return __ddiv_rn(a, c.ko_s2);
-    case 5:  // zo=n-4: planes n-7..n-4 -> q[1..4]
+    default:  // 5: zo=n-4: planes n-7..n-4 -> q[1..4]
       a = ZQ(1); a = mad_rn(a, -3.0, ZQ(2)); a = mad_rn(a, 3.0, ZQ(3)); a = __dsub_rn(a, ZQ(4));
       return __ddiv_rn(a, c.ko_s3);
-    default:
-      return win_ko(q, 4, c);
   }
 }
 #undef ZQ
 
-template <int N>
-__device__ __forceinline__ void q_push(double (&q)[N], double v) {
+template <typename T, int N>
+__device__ __forceinline__ void q_push(T (&q)[N], T v) {
 #pragma unroll
   for (int k = 0; k < N - 1; ++k) q[k] = q[k + 1];
   q[N - 1] = v;
 }
 
-template <typename ST>
-__global__ void __launch_bounds__(kDerivThreads, 2)
-bssn_derivs_kernel(const __grid_constant__ DerivArgs a) {
-  __shared__ double s_plane[2][kPlane];           // staged planes (tile + x-y halo)
-  __shared__ double s_dxp[kDxRows * kTileX];      // D_x of the current plane, y halo rows
-  __shared__ LineScales s_sc[3];
+// Centred-row arithmetic of the derivative kernel, by precision mode.
+//
+// ExactRows (FP64 mode): the reference's operations and order, each rounded
+// (the win_* rows), so every derivative equals the reference's bit for bit.
+//
+// SplitRows (MIXED mode): the split-precision stencil.  Neighbour values enter
+// only through FP64 differences taken before any downcast -- antisymmetric
+// a_k = u(+k) - u(-k) for first derivatives, symmetric s_k = u(+k) + u(-k) - 2u
+// for second derivatives (the centre weight cancels exactly since the weights
+// sum to zero) -- and the weighted sum of the rounded differences runs in FP32,
+// the precision the derivative is stored in.  The Kreiss-Oliger row, a sixth
+// difference that cancels all lower orders, stays in FP64 (from the same
+// symmetric sums, fused multiply-adds allowed).
+struct ExactRows {
+  using D = double;
+  template <typename T, int N>
+  static __device__ __forceinline__ D d1(const T (&w)[N], int C, const LineScales& c) {
+    return win_d1(w, C, c);
+  }
+  // first derivative kept for composition (D_x, D_y fields)
+  template <int N>
+  static __device__ __forceinline__ double d1_field(const double (&w)[N], int C, const LineScales& c) {
+    return win_d1(w, C, c);
+  }
+  template <int N>
+  static __device__ __forceinline__ D d2(const double (&w)[N], int C, const LineScales& c) {
+    return win_d2(w, C, c);
+  }
+  template <int N>
+  static __device__ __forceinline__ double ko(const double (&w)[N], int C, const LineScales& c) {
+    return win_ko(w, C, c);
+  }
+};
 
-  const TileDev t = a.tiles[a.tile_base + blockIdx.x];
+struct SplitRows {
+  using D = float;
+  template <typename T, int N>
+  static __device__ __forceinline__ D d1(const T (&w)[N], int C, const LineScales& c) {
+    const float a1 = (float)(w[C + 1] - w[C - 1]);
+    const float a2 = (float)(w[C + 2] - w[C - 2]);
+    const float a3 = (float)(w[C + 3] - w[C - 3]);
+    return fmaf(45.0f, a1, fmaf(-9.0f, a2, a3)) * (float)c.d1_c;
+  }
+  // D_x / D_y fields that feed the mixed derivatives stay FP64: differencing
+  // FP32-rounded first derivatives would cancel their leading digits
+  template <int N>
+  static __device__ __forceinline__ double d1_field(const double (&w)[N], int C, const LineScales& c) {
+    const double a1 = w[C + 1] - w[C - 1];
+    const double a2 = w[C + 2] - w[C - 2];
+    const double a3 = w[C + 3] - w[C - 3];
+    return fma(45.0, a1, fma(-9.0, a2, a3)) * c.d1_c;
+  }
+  template <int N>
+  static __device__ __forceinline__ D d2(const double (&w)[N], int C, const LineScales& c) {
+    const double u2 = 2.0 * w[C];
+    const float s1 = (float)((w[C + 1] + w[C - 1]) - u2);
+    const float s2 = (float)((w[C + 2] + w[C - 2]) - u2);
+    const float s3 = (float)((w[C + 3] + w[C - 3]) - u2);
+    return fmaf(270.0f, s1, fmaf(-27.0f, s2, 2.0f * s3)) * (float)c.d2_c;
+  }
+  template <int N>
+  static __device__ __forceinline__ double ko(const double (&w)[N], int C, const LineScales& c) {
+    const double u2 = 2.0 * w[C];
+    const double s1 = (w[C + 1] + w[C - 1]) - u2;
+    const double s2 = (w[C + 2] + w[C - 2]) - u2;
+    const double s3 = (w[C + 3] + w[C - 3]) - u2;
+    return c.ko_c * fma(-15.0, s1, fma(6.0, s2, -s3));
+  }
+};
+
+// Closure rows (rare: next to flagged faces) on shared memory, evaluated exactly
+// in FP64; float values (MIXED-mode D_x/D_y fields) are widened first.
+template <typename T>
+static __device__ __noinline__ double cl_d1(const T* p, int s, int pos, int n, bool lo, bool hi,
+                                            const LineScales& c) {
+  double v[9];  // values at pos-4 .. pos+4 that lie inside [0, n)
+#pragma unroll
+  for (int k = 0; k < 9; ++k) {
+    const int at = pos + k - 4;
+    v[k] = (at >= 0 && at < n) ? (double)p[(k - 4) * s] : 0.0;
+  }
+  return line_d1(v + 4, 1, pos, n, lo, hi, c);
+}
+template <typename T>
+static __device__ __noinline__ double cl_d2(const T* p, int s, int pos, int n, bool lo, bool hi,
+                                            const LineScales& c) {
+  double v[9];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) {
+    const int at = pos + k - 4;
+    v[k] = (at >= 0 && at < n) ? (double)p[(k - 4) * s] : 0.0;
+  }
+  return line_d2(v + 4, 1, pos, n, lo, hi, c);
+}
+template <typename T>
+static __device__ __noinline__ double cl_ko(const T* p, int s, int pos, int n, bool lo, bool hi,
+                                            const LineScales& c) {
+  double v[9];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) {
+    const int at = pos + k - 4;
+    v[k] = (at >= 0 && at < n) ? (double)p[(k - 4) * s] : 0.0;
+  }
+  return line_ko(v + 4, 1, pos, n, lo, hi, c);
+}
+
+template <typename ST>
+struct RowsFor { using type = ExactRows; };
+template <>
+struct RowsFor<float> { using type = SplitRows; };
+
+// One (column tile, variable) work item.
+template <typename ST>
+__device__ __forceinline__ void derive_tile(const DerivArgs& a, const TileDev t, const int v,
+                                            double (*s_plane)[kPlane], void* s_dxp_raw,
+                                            LineScales* s_sc) {
+  using Rows = typename RowsFor<ST>::type;
+  double* s_dxp = static_cast<double*>(s_dxp_raw);
   const UnitDev un = a.units[t.unit];
   const BlockDev& B = a.blocks[un.block];
   const int nx = B.sz[0], ny = B.sz[1], nz = B.sz[2];
@@ -219,10 +324,11 @@ bssn_derivs_kernel(const __grid_constant__ DerivArgs a) {
   const int plane_pts = I0 * I1;
   const int lp_col = (int)un.sbase + (gi - 3) + I0 * (gj - 3);  // + plane_pts * (z - k0)
   const int zs = max(0, k0 - kHalo);
-  const int zend = k0 + ez + kHalo;  // exclusive; planes >= nz are not loaded
+  const int zend = k0 + ez + kHalo;  // exclusive
+  const int zload = min(nz, zend);   // planes beyond are never loaded
   const bool clx = closure_row(gi, nx, lox, hix), cly = closure_row(gj, ny, loy, hiy);
 
-  // This thread's share of a plane copy (fixed for the whole CTA): column bx of
+  // This thread's share of a plane copy (fixed for the whole item): column bx of
   // the 32-wide staging grid, rows by0, by0+8, by0+16 of the 24-row plane.
   const int sbx = threadIdx.x & 31, sby0 = threadIdx.x >> 5;
   int st_soff[3], st_goff[3];
@@ -246,110 +352,137 @@ bssn_derivs_kernel(const __grid_constant__ DerivArgs a) {
   }
   const int64_t plane_elems = (int64_t)nx * ny;
 
-  for (int v = 0; v < kNumVars; ++v) {
-    const int q = dd_index(v);
-    const double* __restrict__ f = a.u[v] + B.offset;
-    double qu[kQ], qx[kQ], qy[kQ], qk[kHalo + 1];
+  const int q = dd_index(v);
+  const double* __restrict__ f = a.u[v] + B.offset;
+  double qu[kQ], qx[kQ], qy[kQ];
+  double qk[kHalo + 1];
 #pragma unroll
-    for (int k = 0; k < kQ; ++k) qu[k] = qx[k] = qy[k] = 0.0;
+  for (int k = 0; k < kQ; ++k) qu[k] = qx[k] = qy[k] = 0.0;
 #pragma unroll
-    for (int k = 0; k <= kHalo; ++k) qk[k] = 0.0;
+  for (int k = 0; k <= kHalo; ++k) qk[k] = 0.0;
 
-    // stage plane zi into buffer b (one commit group; empty when zi >= nz)
-    auto stage = [&](int zi, int b) {
-      if (zi < nz) {
-        const double* fp = f + plane_elems * zi;
+  // stage plane zi into buffer b (one commit group; empty past the last needed plane)
+  auto stage = [&](int zi, int b) {
+    if (zi < zload) {
+      const double* fp = f + plane_elems * zi;
 #pragma unroll
-        for (int r = 0; r < 3; ++r)
-          if (st_ok[r]) cp_async8(&s_plane[b][st_soff[r]], fp + st_goff[r]);
+      for (int r = 0; r < 3; ++r)
+        if (st_ok[r]) cp_async8(&s_plane[b][st_soff[r]], fp + st_goff[r]);
+    }
+    cp_async_commit();
+  };
+
+  // Three plane buffers: plane zi+2 streams into the buffer plane zi-1 used,
+  // which every thread has finished with once it passes the barrier of step zi.
+  stage(zs, 0);
+  stage(zs + 1, 1);
+  for (int zi = zs, b = 0; zi < zend; ++zi, b = (b == 2 ? 0 : b + 1)) {
+    cp_async_wait<1>();
+    __syncthreads();
+    stage(zi + 2, b == 0 ? 2 : b - 1);
+    const double* P = s_plane[b];
+    const bool in_block = zi < nz;
+    const bool out_plane = zi >= k0 && zi < k0 + ez;
+    const LineScales& cx = s_sc[0];
+    const LineScales& cy = s_sc[1];
+
+    // D_x of this plane on the tile's x range and the y halo rows (only the
+    // variables with mixed derivatives need the halo rows)
+    if (q >= 0 && in_block) {
+#pragma unroll
+      for (int r = 0; r < 2; ++r) {
+        if (dx_ok[r]) {
+          const int yy = dyy0 + 16 * r;
+          const double* p = P + yy * kPlaneW + dxx + kHalo;
+          double w[7];
+#pragma unroll
+          for (int k = 0; k < 7; ++k) w[k] = p[k - 3];
+          s_dxp[yy * kTileX + dxx] = dcl ? cl_d1(p, 1, dpi, nx, lox, hix, cx) : Rows::d1_field(w, 3, cx);
+        }
       }
-      cp_async_commit();
-    };
-
-    __syncthreads();  // previous variable's readers are done with both buffers
-    stage(zs, 0);
-    for (int zi = zs; zi < zend; ++zi) {
-      const int b = (zi - zs) & 1;
-      stage(zi + 1, b ^ 1);
-      cp_async_wait<1>();
       __syncthreads();
-      const double* P = s_plane[b];
-      const bool in_block = zi < nz;
-      const bool out_plane = zi >= k0 && zi < k0 + ez;
+    }
 
-      // D_x of this plane on the tile's x range and the y halo rows (only the
-      // variables with mixed derivatives need the halo rows).
-      if (q >= 0 && in_block) {
+    double dx = 0.0, dy = 0.0, kxy = 0.0, u0 = 0.0;
+    if (active && in_block) {
+      const double* pc = P + (ty + kHalo) * kPlaneW + (tx + kHalo);
+      u0 = *pc;
+      double wx[7], wy[7];
 #pragma unroll
-        for (int r = 0; r < 2; ++r) {
-          if (dx_ok[r]) {
-            const int yy = dyy0 + 16 * r;
-            const double* p = P + yy * kPlaneW + dxx + kHalo;
-            s_dxp[yy * kTileX + dxx] = dcl ? line_d1_cl(p, 1, dpi, nx, lox, hix, s_sc[0])
-                                           : line_d1(p, 1, dpi, nx, false, false, s_sc[0]);
-          }
-        }
-        __syncthreads();
+      for (int k = 0; k < 7; ++k) {
+        wx[k] = pc[k - 3];
+        wy[k] = pc[(k - 3) * kPlaneW];
       }
-
-      double dx = 0.0, dy = 0.0, kxy = 0.0, u0 = 0.0;
-      if (active && in_block) {
-        const double* pc = P + (ty + kHalo) * kPlaneW + (tx + kHalo);
-        u0 = *pc;
-        double wx[7], wy[7];
-#pragma unroll
-        for (int k = 0; k < 7; ++k) {
-          wx[k] = pc[k - 3];
-          wy[k] = pc[(k - 3) * kPlaneW];
-        }
-        const LineScales& cx = s_sc[0];
-        const LineScales& cy = s_sc[1];
-        dx = q >= 0 ? s_dxp[(ty + kHalo) * kTileX + tx]
-                    : (clx ? line_d1_cl(pc, 1, gi, nx, lox, hix, cx) : win_d1(wx, 3, cx));
-        dy = cly ? line_d1_cl(pc, kPlaneW, gj, ny, loy, hiy, cy) : win_d1(wy, 3, cy);
-        if (out_plane) {
-          const int lp = lp_col + plane_pts * (zi - k0);
-          const double kx = clx ? line_ko_cl(pc, 1, gi, nx, lox, hix, cx) : win_ko(wx, 3, cx);
-          const double ky = cly ? line_ko_cl(pc, kPlaneW, gj, ny, loy, hiy, cy) : win_ko(wy, 3, cy);
-          kxy = __dadd_rn(kx, ky);
-          put_slot<ST>(a, 3 * v + 0, lp, dx);
-          put_slot<ST>(a, 3 * v + 1, lp, dy);
-          if (q >= 0) {
-            const int s0 = 72 + 6 * q;
-            put_slot<ST>(a, s0 + 0, lp, clx ? line_d2_cl(pc, 1, gi, nx, lox, hix, cx) : win_d2(wx, 3, cx));
-            put_slot<ST>(a, s0 + 3, lp, cly ? line_d2_cl(pc, kPlaneW, gj, ny, loy, hiy, cy) : win_d2(wy, 3, cy));
-            const double* pd = s_dxp + (ty + kHalo) * kTileX + tx;
-            double wd[7];
-#pragma unroll
-            for (int k = 0; k < 7; ++k) wd[k] = pd[(k - 3) * kTileX];
-            put_slot<ST>(a, s0 + 1, lp, cly ? line_d1_cl(pd, kTileX, gj, ny, loy, hiy, cy) : win_d1(wd, 3, cy));
-          }
-        }
-      }
-      q_push(qu, u0);
-      q_push(qx, dx);
-      q_push(qy, dy);
-      q_push(qk, kxy);
-
-      // z derivatives of plane zo = zi - 4, whose +-4 neighbourhood is now queued
-      const int zo = zi - kHalo;
-      if (active && zo >= k0 && zo < k0 + ez) {
-        const LineScales& cz = s_sc[2];
-        const int zc = z_case(zo, nz, loz, hiz);
-        const int lp = lp_col + plane_pts * (zo - k0);
-        put_slot<ST>(a, 3 * v + 2, lp, zq_d1(qu, zc, cz));
-        // rhs.cpp:332-369 sums (ko_x + ko_y) + ko_z
-        a.koscr[v * a.cap + lp] = __dadd_rn(qk[0], zq_ko(qu, zc, cz));
+      dx = q >= 0 ? s_dxp[(ty + kHalo) * kTileX + tx]
+                  : (clx ? cl_d1(pc, 1, gi, nx, lox, hix, cx) : Rows::d1_field(wx, 3, cx));
+      dy = cly ? cl_d1(pc, kPlaneW, gj, ny, loy, hiy, cy) : Rows::d1_field(wy, 3, cy);
+      if (out_plane) {
+        const int lp = lp_col + plane_pts * (zi - k0);
+        const double kx = clx ? cl_ko(pc, 1, gi, nx, lox, hix, cx) : Rows::ko(wx, 3, cx);
+        const double ky = cly ? cl_ko(pc, kPlaneW, gj, ny, loy, hiy, cy) : Rows::ko(wy, 3, cy);
+        kxy = __dadd_rn(kx, ky);
+        put_slot<ST>(a, 3 * v + 0, lp, dx);
+        put_slot<ST>(a, 3 * v + 1, lp, dy);
         if (q >= 0) {
           const int s0 = 72 + 6 * q;
-          put_slot<ST>(a, s0 + 5, lp, zq_d2(qu, zc, cz));
-          put_slot<ST>(a, s0 + 2, lp, zq_d1(qx, zc, cz));
-          put_slot<ST>(a, s0 + 4, lp, zq_d1(qy, zc, cz));
+          put_slot<ST>(a, s0 + 0, lp, clx ? cl_d2(pc, 1, gi, nx, lox, hix, cx) : (double)Rows::d2(wx, 3, cx));
+          put_slot<ST>(a, s0 + 3, lp, cly ? cl_d2(pc, kPlaneW, gj, ny, loy, hiy, cy) : (double)Rows::d2(wy, 3, cy));
+          const double* pd = s_dxp + (ty + kHalo) * kTileX + tx;
+          double wd[7];
+#pragma unroll
+          for (int k = 0; k < 7; ++k) wd[k] = pd[(k - 3) * kTileX];
+          put_slot<ST>(a, s0 + 1, lp,
+                       cly ? cl_d1(pd, kTileX, gj, ny, loy, hiy, cy) : (double)Rows::d1(wd, 3, cy));
         }
       }
-      __syncthreads();  // buffer b and s_dxp are rewritten next step
     }
-    cp_async_wait<0>();
+    q_push(qu, u0);
+    q_push(qx, dx);
+    q_push(qy, dy);
+    q_push(qk, kxy);
+
+    // z derivatives of plane zo = zi - 4, whose +-4 neighbourhood is now queued
+    const int zo = zi - kHalo;
+    if (active && zo >= k0 && zo < k0 + ez) {
+      const LineScales& cz = s_sc[2];
+      const int zc = z_case(zo, nz, loz, hiz);
+      const int lp = lp_col + plane_pts * (zo - k0);
+      const bool zcl = zc >= 0;
+      put_slot<ST>(a, 3 * v + 2, lp, zcl ? zq_d1_closure(qu, zc, cz) : (double)Rows::d1(qu, 4, cz));
+      // rhs.cpp:332-369 sums (ko_x + ko_y) + ko_z
+      a.koscr[v * a.cap + lp] = __dadd_rn(qk[0], zcl ? zq_ko_closure(qu, zc, cz) : Rows::ko(qu, 4, cz));
+      if (q >= 0) {
+        const int s0 = 72 + 6 * q;
+        put_slot<ST>(a, s0 + 5, lp, zcl ? (double)zq_d2_closure(qu, zc, cz) : (double)Rows::d2(qu, 4, cz));
+        put_slot<ST>(a, s0 + 2, lp, zcl ? (double)zq_d1_closure(qx, zc, cz) : (double)Rows::d1(qx, 4, cz));
+        put_slot<ST>(a, s0 + 4, lp, zcl ? (double)zq_d1_closure(qy, zc, cz) : (double)Rows::d1(qy, 4, cz));
+      }
+    }
+  }
+  cp_async_wait<0>();
+}
+
+// Persistent derivative kernel: the grid holds as many CTAs as fit on the GPU at
+// once, and each CTA takes the next (tile, variable) item of the chunk from a
+// device counter (the planner lists a chunk's tiles longest first); an item is
+// one variable streamed through one column tile, so the launch ends with a short
+// tail whatever the mix of block sizes.
+template <typename ST>
+__global__ void __launch_bounds__(kDerivThreads, 2)
+bssn_derivs_kernel(const __grid_constant__ DerivArgs a) {
+  __shared__ double s_plane[3][kPlane];            // staged planes (tile + x-y halo)
+  __shared__ double s_dxp[kDxRows * kTileX];       // D_x of the current plane, y halo rows (FP64)
+  __shared__ LineScales s_sc[3];
+  __shared__ int s_item;
+  for (;;) {
+    __syncthreads();  // the previous item is finished with every shared array
+    if (threadIdx.x == 0) s_item = atomicAdd(a.counter, 1);
+    __syncthreads();
+    const int item = s_item;
+    if (item >= a.tile_count * kNumVars) break;
+    // items run tile-major: the longest tiles (listed first) are all taken first
+    derive_tile<ST>(a, a.tiles[a.tile_base + item / kNumVars], item % kNumVars, s_plane, s_dxp,
+                    s_sc);
   }
 }
 

@@ -39,6 +39,15 @@ SIGMA = 0.4
 ALGEBRA_FLOPS_PER_POINT = 2428 + 48 + 10
 DERIV_FLOPS_PER_POINT = 72 * 12 + 33 * 14 + 33 * 12 + 72 * 14
 MIXED_BAR = 1e-6
+# Algorithmic bytes per interior point.  Derivative kernel: reads the 24 state
+# variables over the padded blocks (24 x 8 B x padded/interior points of the
+# batch) and writes the scratch (138 derivative slots x 8 B or 4 B, 24 KO sums x
+# 8 B).  Algebra kernel: reads the state at the point (24 x 8 B) and the scratch,
+# writes 24 x 8 B.
+SCRATCH_BYTES = {"fp64": 138 * 8 + 24 * 8, "mixed": 138 * 4 + 24 * 8}
+# DRAM bytes per interior point of each kernel measured by ncu on a large-block case
+# (profiles/ncu_derivs_algebra_large_blocks.md): derivative / algebra kernel.
+NCU_TRAFFIC_PER_POINT = {"mixed": (1259.2, 1124.6), "fp64": (1850.3, 1792.4)}
 
 
 def _env_int(k, d):
@@ -210,6 +219,8 @@ def main():
                     help="class-proportional block sample for the CPU reference; 0 = enough "
                          "135^3 blocks to give every host core one (min 0.1)")
     ap.add_argument("--chunk-points", type=int, default=0)
+    ap.add_argument("--slab-depth", type=int, default=0)
+    ap.add_argument("--deriv-ctas", type=int, default=0, help="derivative CTAs per SM (0: max)")
     args = ap.parse_args()
 
     world = _env_int("WORLD_SIZE", 1)
@@ -243,7 +254,8 @@ def main():
     rhs = torch.zeros_like(u)
     ctx = sg.Context(local_rank)
     stream = torch.cuda.ExternalStream(ctx.stream)
-    plans = {p: sg.Plan(ctx, blocks, p, args.chunk_points) for p in (sg.FP64, sg.MIXED)}
+    plans = {p: sg.Plan(ctx, blocks, p, args.chunk_points, args.slab_depth, args.deriv_ctas)
+             for p in (sg.FP64, sg.MIXED)}
     params = {p: sg.Params.make(ko_sigma=SIGMA, precision=p) for p in (sg.FP64, sg.MIXED)}
     npts = plans[sg.FP64].points
     U, R = list(u), list(rhs)
@@ -315,6 +327,25 @@ def main():
     alg_tf = ALGEBRA_FLOPS_PER_POINT * npts / (a_ms * 1e-3) / 1e12
     d64, a64 = prof[sg.FP64]
     alg64_tf = ALGEBRA_FLOPS_PER_POINT * npts / (a64 * 1e-3) / 1e12
+    padded = sum(b.npad for b in blocks)
+    read_state = 24 * 8 * padded / npts
+    hbm_peak = None
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as fh:
+            hbm_peak = float(json.load(fh)["hbm_gbs"])
+        peak_src = "measured (MEASURED_PEAKS.json hbm_gbs, copy test)"
+    except Exception:
+        hbm_peak, peak_src = 6650.0, "fallback 6.65 TB/s"
+    nchunks = max(1, plans[sg.MIXED].launches // 2)
+
+    def hbm_roofline(kernel, ms, bytes_per_pt, mode, which):
+        gbs = bytes_per_pt * npts / (ms * 1e-3) / 1e9
+        traffic = NCU_TRAFFIC_PER_POINT[mode][which] * npts / nchunks
+        return {"kernel": kernel, "bound": "hbm", "achieved": round(gbs, 1), "peak": hbm_peak,
+                "unit": "GB/s", "frac": round(gbs / hbm_peak, 4), "traffic": round(traffic),
+                "bytes_per_point": round(bytes_per_pt, 1), "launches_per_step": nchunks,
+                "peak_source": peak_src,
+                "traffic_note": "ncu DRAM bytes/point on a 3.15M-point case x points per launch"}
 
     # end to end through the host API: H2D of the state, evaluate, D2H of the RHS
     e2e = None
@@ -386,14 +417,22 @@ def main():
                               "per_var_max_rel": [float(f"{x:.3g}") for x in per_var_max],
                               "per_var_rms_rel": [float(f"{x:.3g}") for x in per_var_rms]},
             "kernels_ms": {"deriv": round(d_ms, 3), "algebra": round(a_ms, 3)},
-            "roofline": {"kernel": "bssn_algebra_kernel<float>", "bound": "fp32",
-                         "achieved": round(alg_tf, 3), "peak": round(peak32, 2), "unit": "TFLOP/s",
-                         "frac": round(alg_tf / peak32, 4), "traffic": None,
-                         "peak_source": "measured FMA-chain microbenchmark (b200bssn_fma_peak)",
-                         "flops_per_point": ALGEBRA_FLOPS_PER_POINT},
-            "roofline_fp64": {"kernel": "bssn_algebra_kernel<double>", "bound": "fp64",
-                              "achieved": round(alg64_tf, 3), "peak": round(peak64, 2), "unit": "TFLOP/s",
-                              "frac": round(alg64_tf / peak64, 4)},
+            # dominant kernel of the headline (mixed) evaluation: the derivative kernel
+            "roofline": hbm_roofline("bssn_derivs_kernel<float>", d_ms,
+                                     read_state + SCRATCH_BYTES["mixed"], "mixed", 0),
+            "roofline_algebra": dict(
+                hbm_roofline("bssn_algebra_kernel<float,float>", a_ms,
+                             24 * 8 + SCRATCH_BYTES["mixed"] + 24 * 8, "mixed", 1),
+                fp32_tflops=round(alg_tf, 3), fp32_peak=round(peak32, 2),
+                fp32_frac=round(alg_tf / peak32, 4), flops_per_point=ALGEBRA_FLOPS_PER_POINT,
+                fp_peak_source="measured FMA-chain microbenchmark (b200bssn_fma_peak)"),
+            "roofline_fp64": {
+                "derivs": hbm_roofline("bssn_derivs_kernel<double>", d64,
+                                       read_state + SCRATCH_BYTES["fp64"], "fp64", 0),
+                "algebra": dict(hbm_roofline("bssn_algebra_kernel<double,double>", a64,
+                                             24 * 8 + SCRATCH_BYTES["fp64"] + 24 * 8, "fp64", 1),
+                                fp64_tflops=round(alg64_tf, 3), fp64_peak=round(peak64, 2),
+                                fp64_frac=round(alg64_tf / peak64, 4))},
             "gpu_launches": launches,
             "clocks": clock_info,
             "e2e": e2e,

@@ -113,6 +113,18 @@ int b200bssn_rhs(b200bssn_ctx *ctx, double *const *rhs, const double *const *u,
 int b200bssn_plan_create(b200bssn_ctx *ctx, const b200bssn_block *blocks, uint32_t nblocks,
                          uint32_t precision, uint64_t chunk_points, b200bssn_plan **plan);
 int b200bssn_plan_destroy(b200bssn_plan *plan);
+
+/* Tuning knobs of a plan (0 in any field: the default). */
+typedef struct b200bssn_plan_options {
+  uint64_t chunk_points;       /* interior points per kernel pair (scratch size) */
+  uint32_t slab_depth;         /* max interior z planes per work unit (default 48) */
+  uint32_t deriv_ctas_per_sm;  /* resident derivative CTAs per SM (default: as many as fit) */
+} b200bssn_plan_options;
+
+/* b200bssn_plan_create with explicit options (opts may be NULL). */
+int b200bssn_plan_create_ex(b200bssn_ctx *ctx, const b200bssn_block *blocks, uint32_t nblocks,
+                            uint32_t precision, const b200bssn_plan_options *opts,
+                            b200bssn_plan **plan);
 /* Interior points covered by a plan, and the number of kernel launches one
  * evaluation issues. */
 uint64_t b200bssn_plan_points(const b200bssn_plan *plan);

@@ -37,6 +37,25 @@ def _stale(target, deps):
     return any(os.path.getmtime(d) > t for d in deps)
 
 
+SHIM_SRC = os.path.join(PKG, "shim", "bssnrhs_shim.cpp")
+SHIM_LIB = os.path.join(LIBDIR, "libb200bssn_shim.so")
+
+
+def build_shim(force: bool = False) -> str:
+    """libb200bssn_shim.so: the C++ bssnrhs with the reference's signature, linked
+    against libb200bssn.so; its bssn:: globals stay undefined (the host defines them)."""
+    lib = build(force=False)
+    if force or _stale(SHIM_LIB, [SHIM_SRC, lib, os.path.join(REPO, "include", "b200bssn.h")]):
+        cmd = ["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-I", os.path.join(REPO, "include"),
+               SHIM_SRC, "-L", LIBDIR, "-lb200bssn", "-Wl,-rpath,$ORIGIN", "-o", SHIM_LIB + ".tmp"]
+        res = subprocess.run(cmd, capture_output=True, text=True)
+        if res.returncode != 0:
+            sys.stderr.write(res.stdout + res.stderr)
+            raise RuntimeError("g++ failed building libb200bssn_shim.so")
+        os.replace(SHIM_LIB + ".tmp", SHIM_LIB)
+    return SHIM_LIB
+
+
 def build(verbose: bool = False, force: bool = False) -> str:
     os.makedirs(LIBDIR, exist_ok=True)
     srcs = [os.path.join(CSRC, s) for s in SOURCES]
@@ -65,3 +84,4 @@ if __name__ == "__main__":
     ap.add_argument("--force", action="store_true")
     a = ap.parse_args()
     print(build(verbose=a.verbose, force=a.force))
+    print(build_shim(force=a.force))

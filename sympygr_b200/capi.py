@@ -84,6 +84,16 @@ class BlockC(ctypes.Structure):
     ]
 
 
+class PlanOptions(ctypes.Structure):
+    """``b200bssn_plan_options`` (0 = default)."""
+
+    _fields_ = [
+        ("chunk_points", ctypes.c_uint64),
+        ("slab_depth", ctypes.c_uint32),
+        ("deriv_ctas_per_sm", ctypes.c_uint32),
+    ]
+
+
 _lib = None
 
 # (name, restype, argtypes) of every symbol declared in include/b200bssn.h
@@ -100,6 +110,9 @@ SIGNATURES = [
                                     ctypes.c_uint32, ctypes.POINTER(Params)]),
     ("b200bssn_plan_create", ctypes.c_int, [_P, ctypes.POINTER(BlockC), ctypes.c_uint32,
                                             ctypes.c_uint32, ctypes.c_uint64, ctypes.POINTER(_P)]),
+    ("b200bssn_plan_create_ex", ctypes.c_int, [_P, ctypes.POINTER(BlockC), ctypes.c_uint32,
+                                               ctypes.c_uint32, ctypes.POINTER(PlanOptions),
+                                               ctypes.POINTER(_P)]),
     ("b200bssn_plan_destroy", ctypes.c_int, [_P]),
     ("b200bssn_plan_points", ctypes.c_uint64, [_P]),
     ("b200bssn_plan_launches", ctypes.c_uint32, [_P]),
@@ -236,7 +249,7 @@ class Plan:
     """``b200bssn_plan``: descriptors and scratch for a fixed block list."""
 
     def __init__(self, ctx: Context, blocks: Sequence[Block], precision: int = FP64,
-                 chunk_points: int = 0):
+                 chunk_points: int = 0, slab_depth: int = 0, deriv_ctas_per_sm: int = 0):
         lib = load()
         arr = (BlockC * len(blocks))()
         for i, b in enumerate(blocks):
@@ -247,8 +260,10 @@ class Plan:
                 arr[i].pmax[a] = b.pmax[a]
             arr[i].bflag = b.bflag
         h = ctypes.c_void_p()
-        _check(lib.b200bssn_plan_create(ctx.handle, arr, len(blocks), precision, chunk_points,
-                                        ctypes.byref(h)), "b200bssn_plan_create", ctx)
+        opts = PlanOptions(chunk_points, slab_depth, deriv_ctas_per_sm)
+        _check(lib.b200bssn_plan_create_ex(ctx.handle, arr, len(blocks), precision,
+                                           ctypes.byref(opts), ctypes.byref(h)),
+               "b200bssn_plan_create_ex", ctx)
         self.ctx = ctx
         self.handle = h
         self.precision = precision

@@ -260,6 +260,20 @@ const char* b200bssn_last_error(b200bssn_ctx* ctx) { return ctx ? ctx->last_erro
 
 int b200bssn_plan_create(b200bssn_ctx* ctx, const b200bssn_block* blocks, uint32_t nblocks,
                          uint32_t precision, uint64_t chunk_points, b200bssn_plan** out) {
+  b200bssn_plan_options o;
+  std::memset(&o, 0, sizeof(o));
+  o.chunk_points = chunk_points;
+  return b200bssn_plan_create_ex(ctx, blocks, nblocks, precision, &o, out);
+}
+
+int b200bssn_plan_create_ex(b200bssn_ctx* ctx, const b200bssn_block* blocks, uint32_t nblocks,
+                            uint32_t precision, const b200bssn_plan_options* opts,
+                            b200bssn_plan** out) {
+  b200bssn_plan_options o;
+  std::memset(&o, 0, sizeof(o));
+  if (opts) o = *opts;
+  const uint64_t chunk_points = o.chunk_points;
+  const int64_t slab_depth = o.slab_depth ? (int64_t)o.slab_depth : kTileZ;
   if (!ctx || !blocks || !out || nblocks == 0) return B200BSSN_ERR_INVALID_ARGUMENT;
   if (precision != B200BSSN_FP64 && precision != B200BSSN_MIXED) return B200BSSN_ERR_INVALID_ARGUMENT;
   *out = nullptr;
@@ -298,13 +312,13 @@ int b200bssn_plan_create(b200bssn_ctx* ctx, const b200bssn_block* blocks, uint32
     P->span_lo = std::min<uint64_t>(P->span_lo, in.offset);
     P->span_hi = std::max<uint64_t>(P->span_hi, in.offset + npad);
     const int64_t I0 = in.sz[0] - 6, I1 = in.sz[1] - 6, I2 = in.sz[2] - 6;
-    if ((uint64_t)I0 * I1 * kTileZ > (uint64_t)INT32_MAX) {
+    // z-slabs of nearly equal depth (<= slab_depth planes): the derivative kernel
+    // streams each slab plus 4 halo planes on each side
+    const int64_t nslab = (I2 + slab_depth - 1) / slab_depth;
+    if ((uint64_t)I0 * I1 * ((I2 + nslab - 1) / nslab) > (uint64_t)INT32_MAX) {
       delete P;
       return B200BSSN_ERR_INVALID_ARGUMENT;
     }
-    // z-slabs of nearly equal depth (<= kTileZ planes): the derivative kernel
-    // streams each slab plus 4 halo planes on each side
-    const int64_t nslab = (I2 + kTileZ - 1) / kTileZ;
     for (int64_t sl = 0; sl < nslab; ++sl) {
       const int64_t k0 = sl * I2 / nslab, k1 = (sl + 1) * I2 / nslab;
       UnitDev u;
@@ -379,6 +393,7 @@ int b200bssn_plan_create(b200bssn_ctx* ctx, const b200bssn_block* blocks, uint32
         &per_sm, precision == B200BSSN_MIXED ? (const void*)bssn_derivs_kernel<float>
                                              : (const void*)bssn_derivs_kernel<double>,
         kDerivThreads, kDerivSmemBytes);
+    if (o.deriv_ctas_per_sm) per_sm = std::min<int>(per_sm, (int)o.deriv_ctas_per_sm);
     P->deriv_grid = std::max(1, sms * std::max(1, per_sm));
   }
 

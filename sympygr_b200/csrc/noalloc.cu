@@ -38,6 +38,7 @@ constexpr int kNoallocMaxUnits = 1024;
 constexpr int kNoallocMaxTiles = 4096;
 constexpr int kNoallocMaxRanges = 2048;
 constexpr int kMaxDevices = 64;
+constexpr int kNoallocSlab = 48;  // z-slab depth of this path's work units
 
 // byte layout of the fixed array (each part 256-byte aligned)
 constexpr size_t al256(size_t x) { return (x + 255) & ~size_t(255); }
@@ -79,7 +80,7 @@ int setup_device(int dev, void** addr) {
   return B200BSSN_OK;
 }
 
-// Writes the work descriptors of one block (z-slab units of kTileZ planes, x-y
+// Writes the work descriptors of one block (z-slab units of kNoallocSlab planes, x-y
 // tiles, runs of kAlgebraThreads points) -- the layout b200bssn_plan_create
 // builds on the host -- straight into the fixed array.
 __global__ void noalloc_describe(BlockDev blk, BlockDev* blk_out, int* counter, UnitDev* units,
@@ -94,8 +95,8 @@ __global__ void noalloc_describe(BlockDev blk, BlockDev* blk_out, int* counter, 
   for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < n_units; u += gridDim.x * blockDim.x) {
     UnitDev d;
     d.block = 0;
-    d.k0 = u * kTileZ;
-    d.nz = min(kTileZ, I2 - d.k0);
+    d.k0 = u * kNoallocSlab;
+    d.nz = min(kNoallocSlab, I2 - d.k0);
     d.pad = 0;
     d.sbase = (int64_t)I0 * I1 * d.k0;
     units[u] = d;
@@ -137,9 +138,9 @@ extern "C" int b200bssn_rhs_noalloc(double* const* rhs_dev, const double* const*
   if (block->bflag >> 6) return B200BSSN_ERR_INVALID_ARGUMENT;
   const int64_t I0 = block->sz[0] - 6, I1 = block->sz[1] - 6, I2 = block->sz[2] - 6;
   const int64_t npts = I0 * I1 * I2;
-  const int64_t n_units = (I2 + kTileZ - 1) / kTileZ;
+  const int64_t n_units = (I2 + kNoallocSlab - 1) / kNoallocSlab;
   const int64_t tiles_x = (I0 + kTileX - 1) / kTileX, tiles_y = (I1 + kTileY - 1) / kTileY;
-  const int64_t rpu = (I0 * I1 * kTileZ + kAlgebraThreads - 1) / kAlgebraThreads;
+  const int64_t rpu = (I0 * I1 * kNoallocSlab + kAlgebraThreads - 1) / kAlgebraThreads;
   if (npts > kNoallocMaxPoints || n_units > kNoallocMaxUnits ||
       n_units * tiles_x * tiles_y > kNoallocMaxTiles || n_units * rpu > kNoallocMaxRanges)
     return B200BSSN_ERR_SIZE_LIMIT;

@@ -1,7 +1,7 @@
 // Work-plan descriptors shared by the host planner and the kernels.
 //
 // A plan covers a list of octree blocks.  Each block's interior (sz-6)^3 is cut
-// into z-slabs ("units") of at most kTileZ planes; a unit's points are numbered
+// into z-slabs ("units", by default at most 48 planes); a unit's points are numbered
 // compactly, x fastest:  lp = (i-3) + I0*((j-3) + I1*(k-3-k0)).  Units are packed
 // into chunks whose total point count fits the derivative scratch; each chunk is
 // evaluated by one derivative launch (one CTA per 16x16 column tile of a unit,
@@ -14,7 +14,8 @@ namespace b200bssn {
 
 constexpr int kNumVars = 24;
 constexpr int kNumDerivs = 138;  // algebra inputs: 72 first + 66 second derivatives
-constexpr int kTileX = 16, kTileY = 16, kTileZ = 48;
+constexpr int kTileX = 16, kTileY = 16;
+constexpr int kTileZ = 48;       // default z-slab depth (measured best on the 3000-block batch)
 constexpr int kHalo = 4;         // closure rows reach four points inward (z queue: 4 each side)
 constexpr int kDerivThreads = 256;
 constexpr int kAlgebraThreads = 128;

@@ -1,0 +1,51 @@
+// Test driver for the bssnrhs shim: stands in for the host code (it defines the
+// bssn:: globals, as the host's parameters.cpp would), fills one block from a raw
+// input file, calls bssnrhs with the reference's signature, and writes the RHS.
+//   shim_test <in.bin> <out.bin> <n> <pmin> <h> <bflag> <sigma>
+#include <cstdio>
+#include <cstdlib>
+#include <vector>
+
+void bssnrhs(double** uzipVarsRHS, const double** uZipVars, const unsigned int& offset,
+             const double* ptmin, const double* ptmax, const unsigned int* sz,
+             const unsigned int& bflag);
+
+namespace bssn {
+unsigned int BSSN_LAMBDA[4] = {1, 1, 1, 1};
+double BSSN_LAMBDA_F[2] = {1.0, 0.0};
+double ETA_CONST = 2.0;
+double ETA_R0 = 50.0;
+double ETA_DAMPING_EXP = 1.0;
+double KO_DISS_SIGMA = 0.01;
+}  // namespace bssn
+
+int main(int argc, char** argv) {
+  if (argc != 8) return 2;
+  const unsigned n = (unsigned)std::atoi(argv[3]);
+  const double p0 = std::atof(argv[4]), h = std::atof(argv[5]);
+  const unsigned bflag = (unsigned)std::atoi(argv[6]);
+  bssn::KO_DISS_SIGMA = std::atof(argv[7]);
+  const size_t npad = (size_t)n * n * n;
+  std::vector<double> u(24 * npad), r(24 * npad, 0.0);
+  FILE* f = std::fopen(argv[1], "rb");
+  if (!f || std::fread(u.data(), sizeof(double), u.size(), f) != u.size()) return 3;
+  std::fclose(f);
+  const double* up[24];
+  double* rp[24];
+  for (int v = 0; v < 24; ++v) {
+    up[v] = u.data() + v * npad;
+    rp[v] = r.data() + v * npad;
+  }
+  const double pmin[3] = {p0, p0, p0}, pmax[3] = {p0 + (n - 1) * h, p0 + (n - 1) * h, p0 + (n - 1) * h};
+  const unsigned sz[3] = {n, n, n};
+  const unsigned offset = 0;
+  try {
+    bssnrhs(rp, up, offset, pmin, pmax, sz, bflag);
+  } catch (...) {
+    return 4;
+  }
+  f = std::fopen(argv[2], "wb");
+  if (!f || std::fwrite(r.data(), sizeof(double), r.size(), f) != r.size()) return 5;
+  std::fclose(f);
+  return 0;
+}

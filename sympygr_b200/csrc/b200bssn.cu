@@ -16,8 +16,9 @@ using namespace b200bssn;
 struct b200bssn_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
-  // derivative and algebra streams of the chunk pipeline (see launch_plan)
-  cudaStream_t s_deriv = nullptr, s_alg = nullptr;
+  // derivative and algebra streams of the chunk pipeline (see launch_plan), and
+  // the upload / download streams of the pipelined host path
+  cudaStream_t s_deriv = nullptr, s_alg = nullptr, s_h2d = nullptr, s_d2h = nullptr;
   std::string last_error;
   // single-block drop-in path
   double* blk_u = nullptr;    // [24][npad]
@@ -58,6 +59,11 @@ struct b200bssn_plan {
   std::vector<cudaEvent_t> ev_deriv, ev_alg;  // per chunk: derivative / algebra done
   cudaEvent_t ev_fork = nullptr;
   int* d_counters = nullptr;  // per chunk: work counter of the derivative kernel
+  // pipelined host path: element ranges [part[c], part[c+1]) partition the span, one
+  // per chunk, when chunks hold whole blocks in increasing offset order
+  bool host_pipeline = false;
+  std::vector<uint64_t> part;
+  std::vector<cudaEvent_t> ev_in;  // per chunk: upload done
   int deriv_grid = 0;         // resident CTAs of the persistent derivative kernel
   // host-batch staging (allocated on first host call)
   double* st_u = nullptr;
@@ -89,21 +95,8 @@ bool params_ok(const b200bssn_params* p) {
          (p->ghost_policy == B200BSSN_GHOSTS_PRESERVE || p->ghost_policy == B200BSSN_GHOSTS_ZERO);
 }
 
-// Enqueues one evaluation of the plan.
-//
-// With `ev` null and more than one chunk the chunks are pipelined over two
-// internal streams: the derivative kernel of chunk c (stream s_deriv, scratch
-// buffer c%2) runs while the algebra kernel of chunk c-1 (stream s_alg) is still
-// reading the other buffer; event edges keep the order K1(c) -> K2(c) and
-// K2(c-2) -> K1(c), and the caller's stream `s` forks into and joins from the
-// two streams, so the whole evaluation is ordered on `s` (and can be captured
-// into a CUDA graph from `s`).  With `ev` non-null (profiling) everything runs on
-// `s` in order, with events ev[4c+0..3] around chunk c's two kernels.
-int launch_plan(b200bssn_plan* P, double* const* rhs, const double* const* u,
-                const b200bssn_params* prm, cudaStream_t s, cudaEvent_t* ev = nullptr) {
-  b200bssn_ctx* ctx = P->ctx;
-  DerivArgs da;
-  AlgebraArgs aa;
+void make_args(const b200bssn_plan* P, double* const* rhs, const double* const* u,
+               const b200bssn_params* prm, DerivArgs& da, AlgebraArgs& aa) {
   for (int v = 0; v < kNumVars; ++v) {
     da.u[v] = u[v];
     aa.u[v] = u[v];
@@ -122,7 +115,62 @@ int launch_plan(b200bssn_plan* P, double* const* rhs, const double* const* u,
   aa.eta_r0 = prm->eta_r0;
   aa.eta_damping_exp = prm->eta_damping_exp;
   aa.ko_sigma = prm->ko_sigma;
+}
+
+// The two kernels of chunk ci: derivatives on s1, algebra on s2 (the caller
+// orders s2 after s1 when they differ), scratch buffer `buf`.
+int enqueue_chunk(b200bssn_plan* P, DerivArgs da, AlgebraArgs aa, size_t ci, int buf,
+                  cudaStream_t s1, cudaStream_t s2, cudaEvent_t* ev) {
+  b200bssn_ctx* ctx = P->ctx;
+  const ChunkRec& c = P->chunks[ci];
   const bool mixed = P->precision == B200BSSN_MIXED;
+  da.tile_base = c.tile_begin;
+  da.tile_count = c.tile_count;
+  da.counter = P->d_counters + ci;
+  aa.range_base = c.range_begin;
+  da.dscr = P->dscr[buf];
+  aa.dscr = P->dscr[buf];
+  da.koscr = P->koscr[buf];
+  aa.koscr = P->koscr[buf];
+  if (ev) CK(ctx, cudaEventRecord(ev[4 * ci + 0], s1));
+  dim3 g1(std::min(c.tile_count * kNumVars, P->deriv_grid), 1);
+  if (mixed)
+    bssn_derivs_kernel<float><<<g1, kDerivThreads, kDerivSmemBytes, s1>>>(da);
+  else
+    bssn_derivs_kernel<double><<<g1, kDerivThreads, kDerivSmemBytes, s1>>>(da);
+  CK(ctx, cudaGetLastError());
+  if (ev) CK(ctx, cudaEventRecord(ev[4 * ci + 1], s1));
+  if (s1 != s2) {
+    CK(ctx, cudaEventRecord(P->ev_deriv[ci], s1));
+    CK(ctx, cudaStreamWaitEvent(s2, P->ev_deriv[ci], 0));
+  }
+  if (ev) CK(ctx, cudaEventRecord(ev[4 * ci + 2], s2));
+  if (mixed)
+    bssn_algebra_kernel<float, float><<<c.range_count, kAlgebraThreads, 0, s2>>>(aa);
+  else
+    bssn_algebra_kernel<double, double><<<c.range_count, kAlgebraThreads, 0, s2>>>(aa);
+  CK(ctx, cudaGetLastError());
+  if (ev) CK(ctx, cudaEventRecord(ev[4 * ci + 3], s2));
+  if (s1 != s2) CK(ctx, cudaEventRecord(P->ev_alg[ci], s2));
+  return B200BSSN_OK;
+}
+
+// Enqueues one evaluation of the plan.
+//
+// With `ev` null and more than one chunk the chunks are pipelined over two
+// internal streams: the derivative kernel of chunk c (stream s_deriv, scratch
+// buffer c%2) runs while the algebra kernel of chunk c-1 (stream s_alg) is still
+// reading the other buffer; event edges keep the order K1(c) -> K2(c) and
+// K2(c-2) -> K1(c), and the caller's stream `s` forks into and joins from the
+// two streams, so the whole evaluation is ordered on `s` (and can be captured
+// into a CUDA graph from `s`).  With `ev` non-null (profiling) everything runs on
+// `s` in order, with events ev[4c+0..3] around chunk c's two kernels.
+int launch_plan(b200bssn_plan* P, double* const* rhs, const double* const* u,
+                const b200bssn_params* prm, cudaStream_t s, cudaEvent_t* ev = nullptr) {
+  b200bssn_ctx* ctx = P->ctx;
+  DerivArgs da;
+  AlgebraArgs aa;
+  make_args(P, rhs, u, prm, da, aa);
   const size_t nch = P->chunks.size();
   const bool pipelined = ev == nullptr && nch > 1;
   cudaStream_t s1 = pipelined ? ctx->s_deriv : s, s2 = pipelined ? ctx->s_alg : s;
@@ -133,37 +181,9 @@ int launch_plan(b200bssn_plan* P, double* const* rhs, const double* const* u,
     CK(ctx, cudaStreamWaitEvent(s2, P->ev_fork, 0));
   }
   for (size_t ci = 0; ci < nch; ++ci) {
-    const ChunkRec& c = P->chunks[ci];
-    const int buf = pipelined ? (int)(ci & 1) : 0;
-    da.tile_base = c.tile_begin;
-    aa.range_base = c.range_begin;
-    da.dscr = P->dscr[buf];
-    aa.dscr = P->dscr[buf];
-    da.koscr = P->koscr[buf];
-    aa.koscr = P->koscr[buf];
     if (pipelined && ci >= 2) CK(ctx, cudaStreamWaitEvent(s1, P->ev_alg[ci - 2], 0));
-    if (ev) CK(ctx, cudaEventRecord(ev[4 * ci + 0], s));
-    da.tile_count = c.tile_count;
-    da.counter = P->d_counters + ci;
-    dim3 g1(std::min(c.tile_count * kNumVars, P->deriv_grid), 1);
-    if (mixed)
-      bssn_derivs_kernel<float><<<g1, kDerivThreads, kDerivSmemBytes, s1>>>(da);
-    else
-      bssn_derivs_kernel<double><<<g1, kDerivThreads, kDerivSmemBytes, s1>>>(da);
-    CK(ctx, cudaGetLastError());
-    if (ev) CK(ctx, cudaEventRecord(ev[4 * ci + 1], s));
-    if (pipelined) {
-      CK(ctx, cudaEventRecord(P->ev_deriv[ci], s1));
-      CK(ctx, cudaStreamWaitEvent(s2, P->ev_deriv[ci], 0));
-    }
-    if (ev) CK(ctx, cudaEventRecord(ev[4 * ci + 2], s));
-    if (mixed)
-      bssn_algebra_kernel<float, float><<<c.range_count, kAlgebraThreads, 0, s2>>>(aa);
-    else
-      bssn_algebra_kernel<double, double><<<c.range_count, kAlgebraThreads, 0, s2>>>(aa);
-    CK(ctx, cudaGetLastError());
-    if (ev) CK(ctx, cudaEventRecord(ev[4 * ci + 3], s));
-    if (pipelined) CK(ctx, cudaEventRecord(P->ev_alg[ci], s2));
+    const int rc = enqueue_chunk(P, da, aa, ci, pipelined ? (int)(ci & 1) : 0, s1, s2, ev);
+    if (rc != B200BSSN_OK) return rc;
   }
   if (pipelined) CK(ctx, cudaStreamWaitEvent(s, P->ev_alg[nch - 1], 0));
   return B200BSSN_OK;
@@ -230,6 +250,8 @@ int b200bssn_create(b200bssn_ctx** out, int device) {
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->s_deriv, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->s_alg, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->s_h2d, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->s_d2h, cudaStreamNonBlocking);
   if (e != cudaSuccess) rc = fail_cuda(ctx, e, "context setup");
   if (rc == B200BSSN_OK) rc = set_kernel_attributes(ctx);
   if (rc != B200BSSN_OK) {
@@ -250,6 +272,8 @@ int b200bssn_destroy(b200bssn_ctx* ctx) {
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   if (ctx->s_deriv) cudaStreamDestroy(ctx->s_deriv);
   if (ctx->s_alg) cudaStreamDestroy(ctx->s_alg);
+  if (ctx->s_h2d) cudaStreamDestroy(ctx->s_h2d);
+  if (ctx->s_d2h) cudaStreamDestroy(ctx->s_d2h);
   delete ctx;
   return B200BSSN_OK;
 }
@@ -354,6 +378,10 @@ int b200bssn_plan_create_ex(b200bssn_ctx* ctx, const b200bssn_block* blocks, uin
     const BlockDev& B = P->blocks[u.block];
     const int I0 = B.sz[0] - 6, I1 = B.sz[1] - 6;
     const int64_t np = (int64_t)I0 * I1 * u.nz;
+    // a block's units stay in one chunk when the whole block fits in one
+    const int64_t block_pts = (int64_t)I0 * I1 * (B.sz[2] - 6);
+    const bool first_unit = ui == 0 || P->units[ui - 1].block != u.block;
+    if (first_unit && block_pts <= capacity && cur.points + block_pts > capacity) flush();
     if (cur.points + np > capacity) flush();
     u.sbase = cur.points;
     cur.points += np;
@@ -376,6 +404,31 @@ int b200bssn_plan_create_ex(b200bssn_ctx* ctx, const b200bssn_block* blocks, uin
     }
   }
   flush();
+  // Host pipeline partition: chunk c owns elements [part[c], part[c+1]) when the
+  // chunks' blocks are disjoint and in increasing offset order.
+  {
+    std::vector<uint64_t> lo(P->chunks.size(), UINT64_MAX), hi(P->chunks.size(), 0);
+    size_t ci = 0;
+    for (size_t c = 0; c < P->chunks.size(); ++c) {
+      const ChunkRec& ch = P->chunks[c];
+      for (int r = ch.range_begin; r < ch.range_begin + ch.range_count; ++r) {
+        const BlockDev& B = P->blocks[P->units[P->ranges[r].unit].block];
+        const uint64_t np = (uint64_t)B.sz[0] * B.sz[1] * B.sz[2];
+        lo[c] = std::min(lo[c], B.offset);
+        hi[c] = std::max(hi[c], B.offset + np);
+      }
+    }
+    (void)ci;
+    bool ok = P->chunks.size() > 1;
+    for (size_t c = 0; ok && c + 1 < P->chunks.size(); ++c) ok = hi[c] <= lo[c + 1];
+    if (ok) {
+      P->part.resize(P->chunks.size() + 1);
+      P->part[0] = P->span_lo;
+      for (size_t c = 1; c < P->chunks.size(); ++c) P->part[c] = lo[c];
+      P->part[P->chunks.size()] = P->span_hi;
+      P->host_pipeline = true;
+    }
+  }
   // longest tiles first within each chunk (cost ~ planes streamed)
   for (const ChunkRec& c : P->chunks) {
     auto planes = [&](const TileDev& t) {
@@ -412,9 +465,11 @@ int b200bssn_plan_create_ex(b200bssn_ctx* ctx, const b200bssn_block* blocks, uin
   if (e == cudaSuccess) e = cudaMalloc((void**)&P->d_counters, P->chunks.size() * sizeof(int));
   P->ev_deriv.assign(P->chunks.size(), nullptr);
   P->ev_alg.assign(P->chunks.size(), nullptr);
+  P->ev_in.assign(P->chunks.size(), nullptr);
   for (size_t c = 0; c < P->chunks.size() && e == cudaSuccess; ++c) {
     e = cudaEventCreateWithFlags(&P->ev_deriv[c], cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&P->ev_alg[c], cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&P->ev_in[c], cudaEventDisableTiming);
   }
   if (e != cudaSuccess) {
     int rc = fail_cuda(ctx, e, "plan allocation");
@@ -446,6 +501,8 @@ int b200bssn_plan_destroy(b200bssn_plan* P) {
   if (P->ctx && P->ctx->stream) {
     cudaStreamSynchronize(P->ctx->s_deriv);
     cudaStreamSynchronize(P->ctx->s_alg);
+    cudaStreamSynchronize(P->ctx->s_h2d);
+    cudaStreamSynchronize(P->ctx->s_d2h);
   }
   for (int b = 0; b < 2; ++b) {
     cudaFree(P->dscr[b]);
@@ -454,6 +511,8 @@ int b200bssn_plan_destroy(b200bssn_plan* P) {
   for (cudaEvent_t e : P->ev_deriv)
     if (e) cudaEventDestroy(e);
   for (cudaEvent_t e : P->ev_alg)
+    if (e) cudaEventDestroy(e);
+  for (cudaEvent_t e : P->ev_in)
     if (e) cudaEventDestroy(e);
   if (P->ev_fork) cudaEventDestroy(P->ev_fork);
   cudaFree(P->d_counters);
@@ -507,6 +566,53 @@ int b200bssn_plan_profile(b200bssn_plan* P, double* const* rhs_dev, const double
   return rc;
 }
 
+}  // extern "C"
+
+namespace {
+
+// Pipelined host path: per chunk c, the upload of its element range (stream
+// s_h2d), its two kernels (s_deriv, s_alg) and the download of its range of the
+// RHS (s_d2h), with event edges upload(c) -> K1(c) -> K2(c) -> download(c) and
+// K2(c-2) -> K1(c) (scratch reuse).  Uploads, kernels and downloads of different
+// chunks overlap; both copy directions run at once.
+int host_pipelined(b200bssn_plan* P, double* const* rhs, const double* const* u, double* const* rd,
+                   const double* const* ud, const b200bssn_params* prm) {
+  b200bssn_ctx* ctx = P->ctx;
+  DerivArgs da;
+  AlgebraArgs aa;
+  make_args(P, rd, ud, prm, da, aa);
+  const size_t nch = P->chunks.size();
+  cudaStream_t sin = ctx->s_h2d, s1 = ctx->s_deriv, s2 = ctx->s_alg, sout = ctx->s_d2h;
+  CK(ctx, cudaMemsetAsync(P->d_counters, 0, nch * sizeof(int), s1));
+  for (size_t ci = 0; ci < nch; ++ci) {
+    const uint64_t a = P->part[ci], b = P->part[ci + 1];
+    const size_t nb = (size_t)(b - a) * sizeof(double);
+    for (int v = 0; v < kNumVars; ++v) {
+      CK(ctx, cudaMemcpyAsync((void*)(ud[v] + a), u[v] + a, nb, cudaMemcpyHostToDevice, sin));
+      if (prm->ghost_policy == B200BSSN_GHOSTS_PRESERVE)
+        CK(ctx, cudaMemcpyAsync(rd[v] + a, rhs[v] + a, nb, cudaMemcpyHostToDevice, sin));
+      else
+        CK(ctx, cudaMemsetAsync(rd[v] + a, 0, nb, sin));
+    }
+    CK(ctx, cudaEventRecord(P->ev_in[ci], sin));
+    CK(ctx, cudaStreamWaitEvent(s1, P->ev_in[ci], 0));
+    if (ci >= 2) CK(ctx, cudaStreamWaitEvent(s1, P->ev_alg[ci - 2], 0));
+    const int rc = enqueue_chunk(P, da, aa, ci, (int)(ci & 1), s1, s2, nullptr);
+    if (rc != B200BSSN_OK) return rc;
+    CK(ctx, cudaStreamWaitEvent(sout, P->ev_alg[ci], 0));
+    for (int v = 0; v < kNumVars; ++v)
+      CK(ctx, cudaMemcpyAsync(rhs[v] + a, rd[v] + a, nb, cudaMemcpyDeviceToHost, sout));
+  }
+  CK(ctx, cudaStreamSynchronize(sout));
+  CK(ctx, cudaStreamSynchronize(s1));
+  CK(ctx, cudaStreamSynchronize(sin));
+  return B200BSSN_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
 int b200bssn_rhs_plan_host(b200bssn_plan* P, double* const* rhs, const double* const* u,
                            uint64_t n_elems, const b200bssn_params* prm) {
   if (!P || !rhs || !u || !params_ok(prm)) return B200BSSN_ERR_INVALID_ARGUMENT;
@@ -533,6 +639,9 @@ int b200bssn_rhs_plan_host(b200bssn_plan* P, double* const* rhs, const double* c
     // device arrays are shifted so that element `span_lo` lands at the start
     ud[v] = P->st_u + (size_t)v * len - P->span_lo;
     rd[v] = P->st_rhs + (size_t)v * len - P->span_lo;
+  }
+  if (P->host_pipeline) return host_pipelined(P, rhs, u, rd, ud, prm);
+  for (int v = 0; v < kNumVars; ++v) {
     CK(ctx, cudaMemcpyAsync(P->st_u + (size_t)v * len, u[v] + P->span_lo, bytes,
                             cudaMemcpyHostToDevice, s));
     if (prm->ghost_policy == B200BSSN_GHOSTS_PRESERVE)

@@ -131,10 +131,12 @@ def test_chunking_is_bitwise_invariant(ctx):
     assert torch.equal(outs[0], outs[1]) and torch.equal(outs[0], outs[2])
 
 
+@pytest.mark.parametrize("chunk_points", [0, 3000])  # 3000: several chunks, pipelined copies
 @pytest.mark.parametrize("policy", [sg.GHOSTS_PRESERVE, sg.GHOSTS_ZERO])
-def test_batch_host_ghost_policy(ctx, oracle_lib, policy):
+def test_batch_host_ghost_policy(ctx, oracle_lib, policy, chunk_points):
     u, blocks, total = _fake_batch(BATCH[:4], seed=5)
-    plan = sg.Plan(ctx, blocks, sg.FP64)
+    plan = sg.Plan(ctx, blocks, sg.FP64, chunk_points)
+    assert chunk_points == 0 or plan.launches >= 6
     rhs = np.full_like(u, 7.0)
     prm = sg.Params.make(ko_sigma=0.1, ghost_policy=policy)
     plan.rhs_host(list(rhs), list(u), total, prm)
@@ -145,6 +147,13 @@ def test_batch_host_ghost_policy(ctx, oracle_lib, policy):
         seg = rhs[:, b.offset:b.offset + b.npad]
         ghosts = seg[:, ~wl.interior_mask(b).ravel()]
         assert np.all(ghosts == (7.0 if policy == sg.GHOSTS_PRESERVE else 0.0))
+    # elements between blocks follow the same policy
+    inside = np.zeros(total, dtype=bool)
+    for b in blocks:
+        inside[b.offset:b.offset + b.npad] = True
+    lo = min(b.offset for b in blocks)
+    gaps = rhs[:, lo:][:, ~inside[lo:]]
+    assert np.all(gaps == (7.0 if policy == sg.GHOSTS_PRESERVE else 0.0))
     plan.close()
 
 

@@ -146,6 +146,34 @@ int b200bssn_rhs_plan_device(b200bssn_plan *plan, double *const *rhs_dev,
 int b200bssn_rhs_plan_host(b200bssn_plan *plan, double *const *rhs, const double *const *u,
                            uint64_t n_elems, const b200bssn_params *prm);
 
+/* ---- constraints --------------------------------------------------------- */
+
+/* Number of constraint fields: ham, mom0, mom1, mom2 (VAR_CONSTRAINT C_HAM..C_MOM2,
+ * bssn/include/grDef.h:40). */
+#define B200BSSN_NUM_CONSTRAINTS 4
+
+/* Drop-in for physical_constraints (bssn/CodeGen/physcon.cpp:12-15; expressions of
+ * GR/constraints.py:166-177): one block, HOST arrays.  con[c] (c < 4: ham, mom0,
+ * mom1, mom2) receive the constraints at the block's interior points; ghost points
+ * are left untouched.  The reference's Psi4 outputs (C_PSI4_REAL/IMG) are not
+ * computed.  The stencils use each axis' own spacing; the reference uses hx on all
+ * three axes, which is the same on Dendro's cubic blocks.  `precision` selects
+ * FP64 or split-precision stencils with FP32 algebra.  Blocks until done. */
+int b200bssn_physical_constraints(b200bssn_ctx *ctx, double *const *con, const double *const *u,
+                                  uint32_t offset, const double *pmin, const double *pmax,
+                                  const uint32_t *sz, uint32_t bflag, uint32_t precision);
+
+/* Constraints of every block of a plan on DEVICE arrays, in the plan's precision.
+ * con_dev: NULL, or 4 device arrays indexed like u_dev, written at interior points.
+ * block_norms_dev: NULL, or nblocks*8 device doubles, overwritten per block (plan
+ * order) with { sum ham^2, sum mom0^2, sum mom1^2, sum mom2^2, max|ham|, max|mom0|,
+ * max|mom1|, max|mom2| } over the block's interior points; a non-finite constraint
+ * makes its maximum NaN.  At least one of the two must be given.  Asynchronous on
+ * `stream` (NULL: the context stream); no allocation (graph-capturable). */
+int b200bssn_constraints_plan_device(b200bssn_plan *plan, double *const *con_dev,
+                                     const double *const *u_dev, double *block_norms_dev,
+                                     void *stream);
+
 /* ---- allocation-free variant --------------------------------------------- */
 
 /* Largest interior point count b200bssn_rhs_noalloc accepts: 32^3 (a 38^3

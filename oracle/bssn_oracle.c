@@ -360,3 +360,29 @@ void bssn_oracle_derivative_slots(double *slots, const double *const *u, unsigne
   free_arrays(ko, NV);
   free_arrays(d, BSSN_ORACLE_NUM_DERIVS);
 }
+
+/* Hamiltonian and momentum constraints (GR/constraints.py:166-177) at the interior
+ * points of one block, from the derivative arrays bssnrhs materialises. */
+void bssn_oracle_block_constraints(double *const *con, const double *const *u, unsigned int offset,
+                                   const double *pmin, const double *pmax,
+                                   const unsigned int *sz, unsigned int bflag) {
+  const int nx = (int)sz[0], ny = (int)sz[1], nz = (int)sz[2];
+  const long npad = (long)nx * ny * nz;
+  const double h[3] = {(pmax[0] - pmin[0]) / (nx - 1), (pmax[1] - pmin[1]) / (ny - 1),
+                       (pmax[2] - pmin[2]) / (nz - 1)};
+  double **d = alloc_arrays(BSSN_ORACLE_NUM_DERIVS, npad);
+  all_derivatives(d, u, offset, h, sz, bflag);
+#pragma omp parallel for schedule(static)
+  for (int k = 3; k < nz - 3; ++k) {
+    double uv[NV], dv[BSSN_ORACLE_NUM_DERIVS], out[4];
+    for (int j = 3; j < ny - 3; ++j)
+      for (int i = 3; i < nx - 3; ++i) {
+        const long pp = i + (long)nx * (j + (long)ny * k);
+        for (int v = 0; v < NV; ++v) uv[v] = u[v][offset + pp];
+        for (int s = 0; s < BSSN_ORACLE_NUM_DERIVS; ++s) dv[s] = d[s][pp];
+        bssn_oracle_constraints(uv, dv, out);
+        for (int c = 0; c < 4; ++c) con[c][offset + pp] = out[c];
+      }
+  }
+  free_arrays(d, BSSN_ORACLE_NUM_DERIVS);
+}

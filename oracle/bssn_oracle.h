@@ -44,6 +44,16 @@ void bssn_oracle_ko_deriv42_z(double *Du, const double *u, double h, const unsig
 /* Per-point algebra (generated; oracle/bssn_oracle_algebra.c). */
 void bssn_oracle_algebra(const double *u, const double *d, const double *par, double eta, double *out);
 
+/* Per-point Hamiltonian and momentum constraints (generated;
+ * oracle/bssn_oracle_constraints.c): out[4] = ham, mom0, mom1, mom2. */
+void bssn_oracle_constraints(const double *u, const double *d, double *out);
+
+/* Constraints of one block at its interior points: con[c][offset + IDX] for c < 4
+ * (ham, mom0..2), computed from the same derivatives bssnrhs uses. */
+void bssn_oracle_block_constraints(double *const *con, const double *const *u, unsigned int offset,
+                                   const double *pmin, const double *pmax,
+                                   const unsigned int *sz, unsigned int bflag);
+
 /* Whole-block right-hand side with the reference's signature semantics
  * (bssn/include/rhs.h:33-36): reads u[v][offset + IDX], writes the interior
  * [3,n-3)^3 of rhs[v][offset + IDX]; ghosts of rhs are not touched. */

@@ -114,6 +114,19 @@ def oracle_slots(u, blk):
     return out
 
 
+def oracle_constraints(u, blk, con=None):
+    """C restatement of the Hamiltonian and momentum constraints on one block:
+    con[0..3] = ham, mom0, mom1, mom2 at the interior points (others untouched)."""
+    lib = oracle_lib()
+    u = np.ascontiguousarray(u, dtype=np.float64)
+    if con is None:
+        con = np.zeros((4, u.shape[1]))
+    lib.bssn_oracle_block_constraints(_ptrs(con), _ptrs(u), ctypes.c_uint(blk.offset),
+                                      _dbl3(blk.pmin), _dbl3(blk.pmax), _uint3(blk.sz),
+                                      ctypes.c_uint(blk.bflag))
+    return con
+
+
 def _ref(flavour):
     lib = _load(REF_PARITY if flavour == "parity" else REF_FAST)
     lib.ref_bssnrhs_blocks_omp.restype = ctypes.c_double
@@ -138,6 +151,18 @@ def ref_rhs(u, blk, prm=None, rhs=None, flavour="parity"):
     lib.ref_bssnrhs(_ptrs(rhs), _ptrs(u), ctypes.c_uint(blk.offset), _dbl3(blk.pmin),
                     _dbl3(blk.pmax), _uint3(blk.sz), ctypes.c_uint(blk.bflag))
     return rhs
+
+
+def ref_constraints(u, blk, flavour="parity"):
+    """The reference's own physical_constraints (bssn/CodeGen/physcon.cpp:12) on one
+    block: rows ham, mom0, mom1, mom2, psi4_real, psi4_img. The reference uses hx in
+    all three directions, so compare on blocks with equal spacings only."""
+    lib = _ref(flavour)
+    u = np.ascontiguousarray(u, dtype=np.float64)
+    con = np.zeros((6, u.shape[1]))
+    lib.ref_physical_constraints(_ptrs(con), _ptrs(u), ctypes.c_uint(blk.offset), _dbl3(blk.pmin),
+                                 _dbl3(blk.pmax), _uint3(blk.sz), ctypes.c_uint(blk.bflag))
+    return con
 
 
 def ref_blocks_omp(u, rhs, blocks, prm=None, nthreads=0, flavour="fast"):

@@ -9,6 +9,12 @@
 #include <cstring>
 #include "rhs.h"
 
+// The reference's generated constraint evaluator (bssn/CodeGen/physcon.cpp:12-15),
+// compiled unmodified against the declarations in oracle/ref_shim/physcon.h.
+void physical_constraints(double **uZipConVars, const double **uZipVars, const unsigned int &offset,
+                          const double *pmin, const double *pmax, const unsigned int *sz,
+                          const unsigned int &bflag);
+
 extern "C" {
 
 // Sets the bssn:: globals that bssnrhs reads (bssn/src/parameters.cpp:99-109).
@@ -46,6 +52,16 @@ double ref_bssnrhs_blocks_omp(double** rhs, const double** u, int nblocks,
     bssnrhs(rhs, u, off, pmins + 3 * b, pmaxs + 3 * b, szs + 3 * b, bf);
   }
   return omp_get_wtime() - t0;
+}
+
+// Hamiltonian, momentum and Psi4 of one block through the reference's own
+// `physical_constraints`: con[0..5] = ham, mom0, mom1, mom2, psi4_real, psi4_img
+// (bssn/include/grDef.h:40), written at the interior points. Note the reference
+// evaluates every stencil with hx in all three directions (physcon.cpp:188-340).
+void ref_physical_constraints(double** con, const double** u, unsigned int offset,
+                              const double* pmin, const double* pmax, const unsigned int* sz,
+                              unsigned int bflag) {
+  physical_constraints(con, u, offset, pmin, pmax, sz, bflag);
 }
 
 int ref_max_threads(void) { return omp_get_max_threads(); }

@@ -18,7 +18,8 @@ LIBDIR = os.path.join(PKG, "lib")
 LIB = os.path.join(LIBDIR, "libb200bssn.so")
 
 SOURCES = ["b200bssn.cu", "diagnostics.cu", "noalloc.cu"]
-HEADERS = ["rhs_kernels.cuh", "stencils.cuh", "plan_types.h", "generated/bssn_rhs_algebra.cuh"]
+HEADERS = ["rhs_kernels.cuh", "stencils.cuh", "plan_types.h", "constraint_kernels.cuh",
+           "generated/bssn_rhs_algebra.cuh", "generated/bssn_constraints_algebra.cuh"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

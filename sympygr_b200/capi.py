@@ -121,6 +121,10 @@ SIGNATURES = [
     ("b200bssn_plan_profile", ctypes.c_int, [_P, _P, _P, ctypes.POINTER(Params),
                                              ctypes.POINTER(ctypes.c_double),
                                              ctypes.POINTER(ctypes.c_double)]),
+    ("b200bssn_physical_constraints", ctypes.c_int,
+     [_P, _P, _P, ctypes.c_uint32, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
+      ctypes.POINTER(ctypes.c_uint32), ctypes.c_uint32, ctypes.c_uint32]),
+    ("b200bssn_constraints_plan_device", ctypes.c_int, [_P, _P, _P, _P, _P]),
     ("b200bssn_rhs_noalloc", ctypes.c_int, [_P, _P, ctypes.POINTER(BlockC), ctypes.POINTER(Params), _P]),
     ("b200bssn_debug_block_scratch", ctypes.c_int, [_P, _P, ctypes.c_uint64]),
     ("b200bssn_fma_peak", ctypes.c_int, [ctypes.c_int, ctypes.c_uint32, ctypes.POINTER(ctypes.c_double)]),
@@ -152,10 +156,10 @@ def _check(rc: int, what: str, ctx=None):
         raise B200BssnError(rc, what, detail)
 
 
-def _ptr_table(arrays: Sequence) -> ctypes.Array:
-    """24 raw pointers from numpy arrays or torch tensors (data pointer only)."""
-    if len(arrays) != NUM_VARS:
-        raise ValueError("need 24 variable arrays")
+def _ptr_table(arrays: Sequence, n: int = NUM_VARS) -> ctypes.Array:
+    """n (default 24) raw pointers from numpy arrays or torch tensors (data pointer only)."""
+    if len(arrays) != n:
+        raise ValueError(f"need {n} arrays")
     ptrs = []
     for a in arrays:
         if isinstance(a, np.ndarray):
@@ -168,10 +172,11 @@ def _ptr_table(arrays: Sequence) -> ctypes.Array:
             if str(a.dtype) != "torch.float64" or not a.is_contiguous():
                 raise ValueError("variable tensors must be contiguous float64")
             ptrs.append(a.data_ptr())
-    return (ctypes.c_void_p * NUM_VARS)(*ptrs)
+    return (ctypes.c_void_p * n)(*ptrs)
 
 
 NOALLOC_MAX_POINTS = 32768
+NUM_CONSTRAINTS = 4  # ham, mom0, mom1, mom2
 
 
 def block_struct(b: Block) -> BlockC:
@@ -236,6 +241,18 @@ class Context:
         _check(lib.b200bssn_rhs(self.handle, _ptr_table(rhs), _ptr_table(u), int(offset), pm, px,
                                 s, int(bflag), ctypes.byref(params)), "b200bssn_rhs", self)
 
+    def physical_constraints(self, con, u, offset: int, pmin, pmax, sz, bflag: int,
+                             precision: int = FP64):
+        """Drop-in for the reference's ``physical_constraints`` on HOST arrays: `con`
+        is 4 float64 arrays (ham, mom0, mom1, mom2) written at the block's interior."""
+        lib = load()
+        pm = (ctypes.c_double * 3)(*pmin)
+        px = (ctypes.c_double * 3)(*pmax)
+        s = (ctypes.c_uint32 * 3)(*sz)
+        _check(lib.b200bssn_physical_constraints(self.handle, _ptr_table(con, NUM_CONSTRAINTS),
+                                                 _ptr_table(u), int(offset), pm, px, s, int(bflag),
+                                                 int(precision)),
+               "b200bssn_physical_constraints", self)
 
     def debug_block_scratch(self, npts: int) -> np.ndarray:
         """Derivative slots [162, npts] of the last single-block call."""
@@ -267,6 +284,7 @@ class Plan:
         self.ctx = ctx
         self.handle = h
         self.precision = precision
+        self.nblocks = len(blocks)
 
     @property
     def points(self) -> int:
@@ -282,6 +300,22 @@ class Plan:
         _check(load().b200bssn_rhs_plan_device(self.handle, _ptr_table(rhs), _ptr_table(u),
                                                ctypes.byref(params), ctypes.c_void_p(stream or None)),
                "b200bssn_rhs_plan_device", self.ctx)
+
+    def constraints_device(self, u, con=None, block_norms=None, stream: int = 0):
+        """Constraints of every block on device arrays: `con` (4 device arrays or
+        None) receives ham, mom0..2 at interior points; `block_norms` (None or a
+        contiguous float64 device tensor of nblocks*8) receives per block the sums of
+        squares and maxima of |ham|, |mom0..2|.  Asynchronous on `stream`."""
+        cp = _ptr_table(con, NUM_CONSTRAINTS) if con is not None else None
+        npt = None
+        if block_norms is not None:
+            if block_norms.numel() < 8 * self.nblocks or str(block_norms.dtype) != "torch.float64":
+                raise ValueError("block_norms must hold nblocks*8 float64")
+            npt = block_norms.data_ptr()
+        _check(load().b200bssn_constraints_plan_device(self.handle, cp, _ptr_table(u),
+                                                       ctypes.c_void_p(npt),
+                                                       ctypes.c_void_p(stream or None)),
+               "b200bssn_constraints_plan_device", self.ctx)
 
     def profile(self, rhs, u, params: Params):
         """One evaluation with per-launch events: (derivative ms, algebra ms)."""

@@ -33,6 +33,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
 CUDA_OUT = os.path.join(REPO, "sympygr_b200", "csrc", "generated", "bssn_rhs_algebra.cuh")
 C_OUT = os.path.join(REPO, "oracle", "bssn_oracle_algebra.c")
+CUDA_CON_OUT = os.path.join(REPO, "sympygr_b200", "csrc", "generated", "bssn_constraints_algebra.cuh")
+C_CON_OUT = os.path.join(REPO, "oracle", "bssn_oracle_constraints.c")
+CON_NAMES = ["ham", "mom0", "mom1", "mom2"]
+CON_INDEX = {n: i for i, n in enumerate(CON_NAMES)}
 
 PARAM_NAMES = ["lambda0", "lambda1", "lambda2", "lambda3", "lambda_f0", "lambda_f1"]
 
@@ -92,10 +96,12 @@ def _input_binding(sym_name, slots, flavor):
     raise KeyError(sym_name)
 
 
-def emit_staged(stages, printer, slots):
+def emit_staged(stages, printer, slots, out_index=None):
     """CUDA body for the staged capture (staged.py): each stage is CSE'd on its own
     and its values are bound to named locals before the next stage starts; the
-    last stage's outputs go to the sink.  Returns (lines, ops after CSE, temps)."""
+    last stage's outputs go to the sink (index from `out_index`, default the RHS
+    VAR order).  Returns (lines, ops after CSE, temps)."""
+    out_index = OUT_VAR if out_index is None else out_index
     lines = []
     seen_inputs = set()
     nops = ntmp = 0
@@ -125,7 +131,7 @@ def emit_staged(stages, printer, slots):
             nops += sp.count_ops(e)
             bind(e)
             if last:
-                lines.append("  sink.put(%d, %s);  // %s" % (OUT_VAR[sym], printer.doprint(e), sym))
+                lines.append("  sink.put(%d, %s);  // %s" % (out_index[sym], printer.doprint(e), sym))
             else:
                 lines.append("  const RT %s = %s;" % (sym.name, printer.doprint(e)))
                 stage_syms.add(sym)
@@ -141,7 +147,8 @@ def emit_staged(stages, printer, slots):
     return lines, nops, ntmp
 
 
-def emit(prog, printer, flavor, slots):
+def emit(prog, printer, flavor, slots, out_index=None):
+    out_index = OUT_VAR if out_index is None else out_index
     lines = []
     rt = "RT" if flavor == "cuda" else "double"
     nops = 0
@@ -158,7 +165,7 @@ def emit(prog, printer, flavor, slots):
         else:
             _, name, e = item
             nops += sp.count_ops(e)
-            v = OUT_VAR[name]
+            v = out_index[name]
             if flavor == "cuda":
                 lines.append("  sink.put(%d, %s);  // %s" % (v, printer.doprint(e), name))
             else:
@@ -205,6 +212,41 @@ CUDA_HEADER_STAGED = CUDA_HEADER.replace(
     "// sympygr_b200/codegen/staged.py), each stage CSE'd on its own with\n"
     "// sympy.cse(optimizations='basic') and printed by CudaPrinter (a subclass of\n"
     "// dendrosym/code_printer.py:DendroCPrinter).")
+
+CUDA_CON_HEADER = """\
+// GENERATED by sympygr_b200/codegen/gen_bssn_rhs.py -- do not edit by hand.
+//
+// Hamiltonian and momentum constraints of GR/constraints.py:166-177
+// (ham = chi igt^jk R_jk - A_ij A^ij + 2/3 K^2, mom_i), built in the same stages
+// as the right-hand side (inverse metric, Christoffels, CalGt, Ricci tensor; see
+// sympygr_b200/codegen/staged.py), each stage CSE'd with
+// sympy.cse(optimizations='basic') and printed by CudaPrinter.  %(nops)d ops.
+//
+// Interface: as bssn_rhs_algebra; sink.put(c, RT) with c = 0 ham, 1..3 mom0..2.
+#pragma once
+
+namespace b200bssn {
+
+template <typename RT, class In, class Sink>
+__device__ __forceinline__ void bssn_constraints_algebra(const In& in, Sink& sink) {
+"""
+
+C_CON_HEADER = """\
+/* TEST INFRASTRUCTURE ONLY (oracle).
+ * GENERATED by sympygr_b200/codegen/gen_bssn_rhs.py -- do not edit by hand.
+ *
+ * C restatement of the Hamiltonian and momentum constraints of
+ * GR/constraints.py:166-177 (the expressions bssn/CodeGen/physcon.cpp was generated
+ * from), expanded in the state and its derivatives, CSE'd with
+ * sympy.cse(optimizations='basic') and printed in C99 double arithmetic.
+ *
+ *   u[24], d[138]  as bssn_oracle_algebra;   out[4]  ham, mom0, mom1, mom2
+ */
+#include <math.h>
+#include "bssn_oracle.h"
+
+void bssn_oracle_constraints(const double *u, const double *d, double *out) {
+"""
 
 C_HEADER = """\
 /* TEST INFRASTRUCTURE ONLY (oracle).
@@ -254,6 +296,17 @@ def main(argv=None):
 
     CudaPrinter, CPrinter = make_printers(src.load_dendro_c_printer(args.reference))
     slots = src.derivative_slots()
+
+    # constraints, flat (the oracle's C restatement): a fresh GR/constraints.py
+    # import, before the staged capture turns dendro's geometry into symbols
+    con_names, con_exprs = src.capture_constraints(args.reference)
+    crepl, cred = sp.cse(con_exprs, symbols=sp.numbered_symbols("c"), optimizations="basic")
+    cprog = schedule(con_names, crepl, cred)
+    cbody, cnops = emit(cprog, CPrinter(), "c", slots, out_index=CON_INDEX)
+    with open(C_CON_OUT, "w") as f:
+        f.write(C_CON_HEADER)
+        f.write("\n".join(cbody))
+        f.write("\n}\n")
     prog = schedule(names, repl, reduced)
 
     if args.flat_cuda:
@@ -261,11 +314,19 @@ def main(argv=None):
         ntmp = len(repl)
         header = CUDA_HEADER
     else:
-        from .staged import capture_staged
+        from .staged import capture_constraints_staged, capture_staged
 
         stages = capture_staged(args.reference)
         body, nops, ntmp = emit_staged(stages, CudaPrinter(), slots)
         header = CUDA_HEADER_STAGED
+        # constraints: the RHS stages they use (not C3) + their own output stage
+        con_stages = [st for st in stages if st[0] not in ("C3", "out")]
+        con_stages += capture_constraints_staged(args.reference)
+        cbody, cnops, _ = emit_staged(con_stages, CudaPrinter(), slots, out_index=CON_INDEX)
+        with open(CUDA_CON_OUT, "w") as f:
+            f.write(CUDA_CON_HEADER % {"nops": cnops})
+            f.write("\n".join(cbody))
+            f.write("\n}\n\n}  // namespace b200bssn\n")
     os.makedirs(os.path.dirname(CUDA_OUT), exist_ok=True)
     with open(CUDA_OUT, "w") as f:
         f.write(header % {"orig": orig, "nops": nops, "ntmp": ntmp})

@@ -54,6 +54,31 @@ def _chris(name):
     return arr
 
 
+def capture_constraints_staged(reference_root: str):
+    """Hamiltonian and momentum constraints of GR/constraints.py:166-177 with the
+    same stage symbols (igt, C1, C2, CalGt, R; the stage definitions are those of
+    ``capture_staged``).  Returns [(stage_name, defs), ..., ("out", [(name, expr)])]
+    with outputs ham, mom0, mom1, mom2.  Must run after ``capture_staged`` in the
+    same process (it reuses the symbolic dendro state that function leaves)."""
+    import dendro  # GR/dendro.py, already configured with the stage symbols
+
+    Rs = _sym3("R")
+    CalGts = [sp.Symbol(f"CalGt{i}") for i in range(3)]
+    saved = dendro.compute_ricci
+    dendro.compute_ricci = lambda Gt_, chi_: [Rs, None, None, CalGts]
+    try:
+        import importlib
+
+        if "constraints" in sys.modules:
+            con = importlib.reload(sys.modules["constraints"])
+        else:
+            import constraints as con  # GR/constraints.py
+    finally:
+        dendro.compute_ricci = saved
+    outs = [("ham", con.ham)] + [(f"mom{i}", con.mom[i]) for i in range(3)]
+    return [("out", [(n, _rename(sp.sympify(e))) for n, e in outs])]
+
+
 def capture_staged(reference_root: str):
     """Returns a list of stages [(stage_name, [(symbol, expr), ...]), ...]; the last
     stage holds the 24 outputs as (output_name, expr).  Expressions use the plain

@@ -173,3 +173,18 @@ def _rename(expr):
             a, b = sorted((int(a), int(b)))
             frep[f] = sp.Symbol(f"grad2_{a}_{b}_{var.name}")
     return expr.xreplace(frep)
+
+
+def capture_constraints(reference_root: str):
+    """The Hamiltonian and momentum constraints of GR/constraints.py:166-177
+    (``ham``, ``mom``), fully expanded in the state and its derivatives.  Must run
+    before ``staged.capture_staged`` in a process (that function replaces dendro's
+    geometric quantities by symbols)."""
+    gr = os.path.join(reference_root, "GR")
+    if gr not in sys.path:
+        sys.path.insert(0, gr)
+    with contextlib.redirect_stdout(io.StringIO()):
+        import constraints as con  # GR/constraints.py (builds the expressions at import)
+    names = ["ham", "mom0", "mom1", "mom2"]
+    exprs = [con.ham] + [con.mom[i] for i in range(3)]
+    return names, [_rename(sp.sympify(e)) for e in exprs]

@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "b200bssn.h"
+#include "constraint_kernels.cuh"
 #include "rhs_kernels.cuh"
 
 using namespace b200bssn;
@@ -117,10 +118,12 @@ void make_args(const b200bssn_plan* P, double* const* rhs, const double* const* 
   aa.ko_sigma = prm->ko_sigma;
 }
 
-// The two kernels of chunk ci: derivatives on s1, algebra on s2 (the caller
-// orders s2 after s1 when they differ), scratch buffer `buf`.
+// The two kernels of chunk ci: derivatives on s1, then on s2 the algebra or, with
+// `ca` non-null, the constraint kernel (the caller orders s2 after s1 when they
+// differ), scratch buffer `buf`.
 int enqueue_chunk(b200bssn_plan* P, DerivArgs da, AlgebraArgs aa, size_t ci, int buf,
-                  cudaStream_t s1, cudaStream_t s2, cudaEvent_t* ev) {
+                  cudaStream_t s1, cudaStream_t s2, cudaEvent_t* ev,
+                  const ConstraintArgs* ca = nullptr) {
   b200bssn_ctx* ctx = P->ctx;
   const ChunkRec& c = P->chunks[ci];
   const bool mixed = P->precision == B200BSSN_MIXED;
@@ -145,10 +148,19 @@ int enqueue_chunk(b200bssn_plan* P, DerivArgs da, AlgebraArgs aa, size_t ci, int
     CK(ctx, cudaStreamWaitEvent(s2, P->ev_deriv[ci], 0));
   }
   if (ev) CK(ctx, cudaEventRecord(ev[4 * ci + 2], s2));
-  if (mixed)
+  if (ca) {
+    ConstraintArgs cc = *ca;
+    cc.range_base = c.range_begin;
+    cc.dscr = P->dscr[buf];
+    if (mixed)
+      bssn_constraints_kernel<float, float><<<c.range_count, kAlgebraThreads, 0, s2>>>(cc);
+    else
+      bssn_constraints_kernel<double, double><<<c.range_count, kAlgebraThreads, 0, s2>>>(cc);
+  } else if (mixed) {
     bssn_algebra_kernel<float, float><<<c.range_count, kAlgebraThreads, 0, s2>>>(aa);
-  else
+  } else {
     bssn_algebra_kernel<double, double><<<c.range_count, kAlgebraThreads, 0, s2>>>(aa);
+  }
   CK(ctx, cudaGetLastError());
   if (ev) CK(ctx, cudaEventRecord(ev[4 * ci + 3], s2));
   if (s1 != s2) CK(ctx, cudaEventRecord(P->ev_alg[ci], s2));
@@ -165,8 +177,12 @@ int enqueue_chunk(b200bssn_plan* P, DerivArgs da, AlgebraArgs aa, size_t ci, int
 // two streams, so the whole evaluation is ordered on `s` (and can be captured
 // into a CUDA graph from `s`).  With `ev` non-null (profiling) everything runs on
 // `s` in order, with events ev[4c+0..3] around chunk c's two kernels.
+//
+// With `ca` non-null the second kernel of every chunk is the constraint kernel
+// (`rhs` and `prm` are then only used to fill the unused algebra arguments).
 int launch_plan(b200bssn_plan* P, double* const* rhs, const double* const* u,
-                const b200bssn_params* prm, cudaStream_t s, cudaEvent_t* ev = nullptr) {
+                const b200bssn_params* prm, cudaStream_t s, cudaEvent_t* ev = nullptr,
+                const ConstraintArgs* ca = nullptr) {
   b200bssn_ctx* ctx = P->ctx;
   DerivArgs da;
   AlgebraArgs aa;
@@ -182,7 +198,7 @@ int launch_plan(b200bssn_plan* P, double* const* rhs, const double* const* u,
   }
   for (size_t ci = 0; ci < nch; ++ci) {
     if (pipelined && ci >= 2) CK(ctx, cudaStreamWaitEvent(s1, P->ev_alg[ci - 2], 0));
-    const int rc = enqueue_chunk(P, da, aa, ci, pipelined ? (int)(ci & 1) : 0, s1, s2, ev);
+    const int rc = enqueue_chunk(P, da, aa, ci, pipelined ? (int)(ci & 1) : 0, s1, s2, ev, ca);
     if (rc != B200BSSN_OK) return rc;
   }
   if (pipelined) CK(ctx, cudaStreamWaitEvent(s, P->ev_alg[nch - 1], 0));
@@ -659,13 +675,17 @@ int b200bssn_rhs_plan_host(b200bssn_plan* P, double* const* rhs, const double* c
   return B200BSSN_OK;
 }
 
-int b200bssn_rhs(b200bssn_ctx* ctx, double* const* rhs, const double* const* u, uint32_t offset,
-                 const double* pmin, const double* pmax, const uint32_t* sz, uint32_t bflag,
-                 const b200bssn_params* prm) {
-  if (!ctx || !rhs || !u || !pmin || !pmax || !sz || !params_ok(prm))
-    return B200BSSN_ERR_INVALID_ARGUMENT;
-  for (int v = 0; v < kNumVars; ++v)
-    if (!rhs[v] || !u[v]) return B200BSSN_ERR_INVALID_ARGUMENT;
+}  // extern "C"
+
+namespace {
+
+// Single-block path shared by the drop-in entry points: (re)builds the one-block
+// plan when the size or precision changes (otherwise only the block descriptor is
+// refreshed), sizes the block buffers and uploads the block's state.  On return
+// ud/rd point at the device copies of u and at a [24][npad] output buffer.
+int prepare_block(b200bssn_ctx* ctx, const double* const* u, uint32_t offset, const double* pmin,
+                  const double* pmax, const uint32_t* sz, uint32_t bflag, uint32_t precision,
+                  const double** ud, double** rd) {
   CK(ctx, cudaSetDevice(ctx->device));
   b200bssn_block blk;
   blk.offset = 0;
@@ -676,24 +696,24 @@ int b200bssn_rhs(b200bssn_ctx* ctx, double* const* rhs, const double* const* u, 
     blk.pmax[a] = pmax[a];
   }
   const size_t npad = (size_t)sz[0] * sz[1] * sz[2];
-  // (re)build the one-block plan when the size or precision changes; otherwise
-  // only the block descriptor (corners, flags) is refreshed.
   if (!ctx->blk_plan || std::memcmp(ctx->blk_sz, sz, sizeof(ctx->blk_sz)) != 0 ||
-      ctx->blk_precision != prm->precision) {
+      ctx->blk_precision != precision) {
     if (ctx->blk_plan) b200bssn_plan_destroy(ctx->blk_plan);
     ctx->blk_plan = nullptr;
-    int rc = b200bssn_plan_create(ctx, &blk, 1, prm->precision, 0, &ctx->blk_plan);
+    int rc = b200bssn_plan_create(ctx, &blk, 1, precision, 0, &ctx->blk_plan);
     if (rc != B200BSSN_OK) return rc;
     std::memcpy(ctx->blk_sz, sz, sizeof(ctx->blk_sz));
-    ctx->blk_precision = prm->precision;
+    ctx->blk_precision = precision;
   } else {
+    if (bflag >> 6) return B200BSSN_ERR_INVALID_ARGUMENT;
+    for (int a = 0; a < 3; ++a)
+      if (!(pmax[a] > pmin[a])) return B200BSSN_ERR_INVALID_ARGUMENT;
     BlockDev& d = ctx->blk_plan->blocks[0];
     d.bflag = bflag;
     for (int a = 0; a < 3; ++a) {
       d.pmin[a] = pmin[a];
       d.h[a] = (pmax[a] - pmin[a]) / (sz[a] - 1);
     }
-    if (bflag >> 6) return B200BSSN_ERR_INVALID_ARGUMENT;
     CK(ctx, cudaMemcpyAsync(ctx->blk_plan->d_blocks, &d, sizeof(BlockDev), cudaMemcpyHostToDevice,
                             ctx->stream));
   }
@@ -706,32 +726,113 @@ int b200bssn_rhs(b200bssn_ctx* ctx, double* const* rhs, const double* const* u, 
     CK(ctx, cudaMalloc((void**)&ctx->blk_rhs, kNumVars * npad * sizeof(double)));
     ctx->blk_cap = npad;
   }
-  cudaStream_t s = ctx->stream;
-  const double* ud[kNumVars];
-  double* rd[kNumVars];
   for (int v = 0; v < kNumVars; ++v) {
     ud[v] = ctx->blk_u + v * npad;
     rd[v] = ctx->blk_rhs + v * npad;
     CK(ctx, cudaMemcpyAsync((void*)ud[v], u[v] + offset, npad * sizeof(double),
-                            cudaMemcpyHostToDevice, s));
+                            cudaMemcpyHostToDevice, ctx->stream));
   }
-  int rc = launch_plan(ctx->blk_plan, rd, ud, prm, s);
-  if (rc != B200BSSN_OK) return rc;
-  // copy back the interior box only: the reference leaves ghost points untouched
+  return B200BSSN_OK;
+}
+
+// Copies the interior box [3, n-3)^3 of `nout` device arrays back to the caller's
+// host arrays at `offset`; ghost points of the destination are left untouched, as
+// the reference leaves them.
+int copy_interior_back(b200bssn_ctx* ctx, double* const* dst, double* const* src, int nout,
+                       uint32_t offset, const uint32_t* sz) {
   const size_t nx = sz[0], ny = sz[1];
-  for (int v = 0; v < kNumVars; ++v) {
+  for (int v = 0; v < nout; ++v) {
     cudaMemcpy3DParms cp;
     std::memset(&cp, 0, sizeof(cp));
-    cp.srcPtr = make_cudaPitchedPtr(rd[v], nx * sizeof(double), nx, ny);
-    cp.dstPtr = make_cudaPitchedPtr(rhs[v] + offset, nx * sizeof(double), nx, ny);
+    cp.srcPtr = make_cudaPitchedPtr(src[v], nx * sizeof(double), nx, ny);
+    cp.dstPtr = make_cudaPitchedPtr(dst[v] + offset, nx * sizeof(double), nx, ny);
     cp.srcPos = make_cudaPos(3 * sizeof(double), 3, 3);
     cp.dstPos = cp.srcPos;
     cp.extent = make_cudaExtent((nx - 6) * sizeof(double), ny - 6, sz[2] - 6);
     cp.kind = cudaMemcpyDeviceToHost;
-    CK(ctx, cudaMemcpy3DAsync(&cp, s));
+    CK(ctx, cudaMemcpy3DAsync(&cp, ctx->stream));
   }
-  CK(ctx, cudaStreamSynchronize(s));
+  CK(ctx, cudaStreamSynchronize(ctx->stream));
   return B200BSSN_OK;
+}
+
+ConstraintArgs constraint_args(const b200bssn_plan* P, double* const* con,
+                               const double* const* u, double* norms) {
+  ConstraintArgs ca;
+  std::memset(&ca, 0, sizeof(ca));
+  for (int v = 0; v < kNumVars; ++v) ca.u[v] = u[v];
+  for (int c = 0; c < kNumConstraints; ++c) ca.con[c] = con ? con[c] : nullptr;
+  ca.norms = norms;
+  ca.blocks = P->d_blocks;
+  ca.units = P->d_units;
+  ca.ranges = P->d_ranges;
+  ca.cap = (int32_t)P->cap;
+  return ca;
+}
+
+}  // namespace
+
+extern "C" {
+
+int b200bssn_rhs(b200bssn_ctx* ctx, double* const* rhs, const double* const* u, uint32_t offset,
+                 const double* pmin, const double* pmax, const uint32_t* sz, uint32_t bflag,
+                 const b200bssn_params* prm) {
+  if (!ctx || !rhs || !u || !pmin || !pmax || !sz || !params_ok(prm))
+    return B200BSSN_ERR_INVALID_ARGUMENT;
+  for (int v = 0; v < kNumVars; ++v)
+    if (!rhs[v] || !u[v]) return B200BSSN_ERR_INVALID_ARGUMENT;
+  const double* ud[kNumVars];
+  double* rd[kNumVars];
+  int rc = prepare_block(ctx, u, offset, pmin, pmax, sz, bflag, prm->precision, ud, rd);
+  if (rc != B200BSSN_OK) return rc;
+  rc = launch_plan(ctx->blk_plan, rd, ud, prm, ctx->stream);
+  if (rc != B200BSSN_OK) return rc;
+  return copy_interior_back(ctx, rhs, rd, kNumVars, offset, sz);
+}
+
+int b200bssn_physical_constraints(b200bssn_ctx* ctx, double* const* con, const double* const* u,
+                                  uint32_t offset, const double* pmin, const double* pmax,
+                                  const uint32_t* sz, uint32_t bflag, uint32_t precision) {
+  if (!ctx || !con || !u || !pmin || !pmax || !sz) return B200BSSN_ERR_INVALID_ARGUMENT;
+  if (precision != B200BSSN_FP64 && precision != B200BSSN_MIXED) return B200BSSN_ERR_INVALID_ARGUMENT;
+  for (int v = 0; v < kNumVars; ++v)
+    if (!u[v]) return B200BSSN_ERR_INVALID_ARGUMENT;
+  for (int c = 0; c < kNumConstraints; ++c)
+    if (!con[c]) return B200BSSN_ERR_INVALID_ARGUMENT;
+  const double* ud[kNumVars];
+  double* rd[kNumVars];
+  int rc = prepare_block(ctx, u, offset, pmin, pmax, sz, bflag, precision, ud, rd);
+  if (rc != B200BSSN_OK) return rc;
+  b200bssn_params prm;
+  b200bssn_default_params(&prm);
+  prm.precision = precision;
+  const ConstraintArgs ca = constraint_args(ctx->blk_plan, rd, ud, nullptr);
+  rc = launch_plan(ctx->blk_plan, rd, ud, &prm, ctx->stream, nullptr, &ca);
+  if (rc != B200BSSN_OK) return rc;
+  return copy_interior_back(ctx, con, rd, kNumConstraints, offset, sz);
+}
+
+int b200bssn_constraints_plan_device(b200bssn_plan* P, double* const* con_dev,
+                                     const double* const* u_dev, double* block_norms_dev,
+                                     void* stream) {
+  if (!P || !u_dev || (!con_dev && !block_norms_dev)) return B200BSSN_ERR_INVALID_ARGUMENT;
+  for (int v = 0; v < kNumVars; ++v)
+    if (!u_dev[v]) return B200BSSN_ERR_INVALID_ARGUMENT;
+  if (con_dev)
+    for (int c = 0; c < kNumConstraints; ++c)
+      if (!con_dev[c]) return B200BSSN_ERR_INVALID_ARGUMENT;
+  b200bssn_ctx* ctx = P->ctx;
+  CK(ctx, cudaSetDevice(ctx->device));
+  cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+  if (block_norms_dev)
+    CK(ctx, cudaMemsetAsync(block_norms_dev, 0,
+                            P->blocks.size() * 2 * kNumConstraints * sizeof(double), s));
+  b200bssn_params prm;
+  b200bssn_default_params(&prm);
+  prm.precision = P->precision;
+  const ConstraintArgs ca = constraint_args(P, con_dev, u_dev, block_norms_dev);
+  // the algebra arguments are unused on this path; u stands in for the rhs arrays
+  return launch_plan(P, const_cast<double* const*>(u_dev), u_dev, &prm, s, nullptr, &ca);
 }
 
 int b200bssn_debug_block_scratch(b200bssn_ctx* ctx, double* slots, uint64_t npts) {

@@ -1,0 +1,126 @@
+// Hamiltonian and momentum constraints on the derivative scratch.
+//
+// The reference evaluates the constraints on the CPU in `physical_constraints`
+// (bssn/CodeGen/physcon.cpp:12-1398, generated from GR/constraints.py:166-177): it
+// materialises first derivatives of chi, Gt, K, gt, At and second derivatives of gt
+// and chi with the same 6th-order operators as bssnrhs, then evaluates
+//   ham   = chi igt^jk R_jk - A_ij A^ij + 2/3 K^2
+//   mom_i = ...                                   (GR/constraints.py:170-177)
+// at every interior point. Here the derivatives come from the derivative kernel
+// (bssn_derivs_kernel, whose 138 slots include all 93 the constraints read), and
+// one thread per interior point runs the generated constraint algebra
+// (generated/bssn_constraints_algebra.cuh).
+//
+// Outputs, each optional: the four constraint fields at the interior points of the
+// caller's arrays (indexed like the state), and per block the sums of squares and
+// the maxima of |ham|, |mom0..2| over its interior points (8 doubles per block,
+// accumulated with one atomic per CTA and constraint; a non-finite value makes the
+// maximum NaN, so the norms double as a finiteness check).
+#pragma once
+
+#include "plan_types.h"
+#include "generated/bssn_constraints_algebra.cuh"
+
+namespace b200bssn {
+
+constexpr int kNumConstraints = 4;  // ham, mom0, mom1, mom2
+
+struct ConstraintArgs {
+  const double* u[kNumVars];
+  double* con[kNumConstraints];  // all null: fields not written
+  double* norms;                 // [nblocks][8] or null
+  const BlockDev* blocks;
+  const UnitDev* units;
+  const RangeDev* ranges;
+  const void* dscr;
+  int32_t cap;
+  int32_t range_base;
+};
+
+template <typename RT, typename ST>
+struct ConstraintIn {
+  const ConstraintArgs* a;
+  int64_t pp;
+  int lp;
+  __device__ __forceinline__ RT u(int v) const { return (RT)__ldg(a->u[v] + pp); }
+  __device__ __forceinline__ RT d(int s) const {
+    return (RT)__ldg(static_cast<const ST*>(a->dscr) + s * a->cap + lp);
+  }
+};
+
+template <typename RT>
+struct ConstraintSink {
+  RT val[kNumConstraints];
+  __device__ __forceinline__ void put(int c, RT v) { val[c] = v; }
+};
+
+// non-negative doubles (and NaN with the sign bit clear) order like their bit patterns
+__device__ __forceinline__ void atomic_max_nonneg(double* addr, double v) {
+  atomicMax(reinterpret_cast<unsigned long long*>(addr),
+            (unsigned long long)__double_as_longlong(v));
+}
+
+template <typename RT, typename ST>
+__global__ void __launch_bounds__(kAlgebraThreads)
+bssn_constraints_kernel(const __grid_constant__ ConstraintArgs a) {
+  const RangeDev rg = a.ranges[a.range_base + blockIdx.x];
+  const UnitDev un = a.units[rg.unit];
+  const BlockDev& B = a.blocks[un.block];
+  const bool active = (int)threadIdx.x < rg.count;
+  double sq[kNumConstraints] = {0.0, 0.0, 0.0, 0.0};
+  double mx[kNumConstraints] = {0.0, 0.0, 0.0, 0.0};
+  if (active) {
+    const int nx = B.sz[0], ny = B.sz[1];
+    const int I0 = nx - 6, I1 = ny - 6;
+    const int lpu = rg.start + threadIdx.x;
+    const int lx = lpu % I0, rr = lpu / I0, ly = rr % I1, lz = rr / I1;
+    const int64_t pp =
+        B.offset + (lx + 3) + (int64_t)nx * ((ly + 3) + (int64_t)ny * (lz + 3 + un.k0));
+    ConstraintIn<RT, ST> in{&a, pp, (int)un.sbase + lpu};
+    ConstraintSink<RT> sink;
+    bssn_constraints_algebra<RT>(in, sink);
+#pragma unroll
+    for (int c = 0; c < kNumConstraints; ++c) {
+      const double v = (double)sink.val[c];
+      if (a.con[c]) a.con[c][pp] = v;
+      sq[c] = v * v;
+      mx[c] = fabs(v);
+    }
+  }
+  if (!a.norms) return;
+  // CTA reduction: warp shuffles, then one value per warp through shared memory
+  __shared__ double s_red[kAlgebraThreads / 32][2 * kNumConstraints];
+#pragma unroll
+  for (int c = 0; c < kNumConstraints; ++c) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      sq[c] += __shfl_xor_sync(0xffffffffu, sq[c], o);
+      const double m = __shfl_xor_sync(0xffffffffu, mx[c], o);
+      mx[c] = (m > mx[c] || m != m) ? m : mx[c];
+    }
+  }
+  const int w = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0) {
+#pragma unroll
+    for (int c = 0; c < kNumConstraints; ++c) {
+      s_red[w][c] = sq[c];
+      s_red[w][kNumConstraints + c] = mx[c];
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < 2 * kNumConstraints) {
+    const int c = threadIdx.x;
+    double r = s_red[0][c];
+    for (int k = 1; k < kAlgebraThreads / 32; ++k) {
+      const double t = s_red[k][c];
+      r = c < kNumConstraints ? r + t : ((t > r || t != t) ? t : r);
+    }
+    double* dst = a.norms + (size_t)un.block * (2 * kNumConstraints) + c;
+    if (c < kNumConstraints)
+      atomicAdd(dst, r);
+    else
+      atomic_max_nonneg(dst, fabs(r));
+  }
+}
+
+}  // namespace b200bssn

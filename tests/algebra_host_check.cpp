@@ -1,6 +1,7 @@
 // Host build of the generated device algebra (sympygr_b200/csrc/generated/
-// bssn_rhs_algebra.cuh) next to the oracle's C algebra, at seeded random points.
-// Prints the largest norm-wise relative difference per output over all points.
+// bssn_rhs_algebra.cuh, or with a second argument "con" the constraint algebra
+// bssn_constraints_algebra.cuh) next to the oracle's C functions, at seeded random
+// points. Prints the largest norm-wise relative difference per output over all points.
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -8,8 +9,11 @@
 #define __device__
 #define __forceinline__ inline
 using std::sqrt;
+#include <cstring>
+#include "bssn_constraints_algebra.cuh"
 #include "bssn_rhs_algebra.cuh"
 extern "C" void bssn_oracle_algebra(const double*, const double*, const double*, double, double*);
+extern "C" void bssn_oracle_constraints(const double*, const double*, double*);
 struct In {
   const double* u_;
   const double* d_;
@@ -22,6 +26,8 @@ struct Sink {
 };
 int main(int argc, char** argv) {
   const int npts = argc > 1 ? std::atoi(argv[1]) : 2000;
+  const bool con = argc > 2 && std::strcmp(argv[2], "con") == 0;
+  const int nout = con ? 4 : 24;
   std::mt19937_64 g(12345);
   std::uniform_real_distribution<double> U(-0.3, 0.3);
   double maxdiff[24] = {0}, maxref[24] = {0};
@@ -39,13 +45,18 @@ int main(int argc, char** argv) {
     const double eta = 2.0 + U(g);
     In in{u, d};
     Sink s{a};
-    b200bssn::bssn_rhs_algebra<double>(in, s, prm, eta);
-    bssn_oracle_algebra(u, d, par, eta, b);
-    for (int v = 0; v < 24; ++v) {
+    if (con) {
+      b200bssn::bssn_constraints_algebra<double>(in, s);
+      bssn_oracle_constraints(u, d, b);
+    } else {
+      b200bssn::bssn_rhs_algebra<double>(in, s, prm, eta);
+      bssn_oracle_algebra(u, d, par, eta, b);
+    }
+    for (int v = 0; v < nout; ++v) {
       maxdiff[v] = std::fmax(maxdiff[v], std::fabs(a[v] - b[v]));
       maxref[v] = std::fmax(maxref[v], std::fabs(b[v]));
     }
   }
-  for (int v = 0; v < 24; ++v) std::printf("%d %.6e\n", v, maxdiff[v] / std::fmax(maxref[v], 1e-300));
+  for (int v = 0; v < nout; ++v) std::printf("%d %.6e\n", v, maxdiff[v] / std::fmax(maxref[v], 1e-300));
   return 0;
 }

@@ -10,6 +10,12 @@ seeded inputs and stores its outputs:
                          per-variable checksums plus 2048 sampled interior points
 * bl_134.npz             the 134^3 Brill-Lindquist block (all faces flagged,
                          sigma=0.4): checksums plus 2048 sampled interior points
+* con_fake_<n>_b<flag>.npz  Hamiltonian and momentum constraints (rows ham, mom0,
+                         mom1, mom2) at the interior of a fake_initial_data block,
+                         from the reference's physical_constraints
+                         (bssn/CodeGen/physcon.cpp:12)
+* con_bl_70.npz          the same on a 70^3 Brill-Lindquist block: checksums plus
+                         2048 sampled interior points
 
 Each file also records the generator parameters and a SHA-256 of the input
 arrays, so a test can verify it regenerated the same inputs.
@@ -76,6 +82,19 @@ def main():
                             input_sha=sha(u), checksums=checksums(ri), sample_index=idx,
                             sample_rhs=ri[:, idx])
         print(name, blk.sz, hex(blk.bflag))
+    for n, pmin, h, bflag in (FAKE_CASES[0], FAKE_CASES[3]):
+        u, blk = po.fake_block(n, pmin, h, bflag)
+        c = po.interior(po.ref_constraints(u, blk), blk)[:4]
+        np.savez_compressed(os.path.join(HERE, f"con_fake_{n}_b{bflag:02x}.npz"),
+                            n=n, pmin=np.array(pmin), h=h, bflag=bflag, input_sha=sha(u),
+                            con_interior=c)
+        print("constraints fake", n, hex(bflag))
+    u, blk = wl.brill_lindquist(70, 8.0, 1.0)
+    c = po.interior(po.ref_constraints(u, blk), blk)[:4]
+    idx = sample_index(c.shape[1], 3)
+    np.savez_compressed(os.path.join(HERE, "con_bl_70.npz"), bflag=blk.bflag, input_sha=sha(u),
+                        checksums=checksums(c), sample_index=idx, sample_con=c[:, idx])
+    print("constraints bl_70", blk.sz)
 
 
 if __name__ == "__main__":

@@ -6,18 +6,36 @@ import os
 import subprocess
 
 import numpy as np
+import pytest
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(HERE)
 
 
-def test_staged_device_algebra_matches_oracle(tmp_path):
-    exe = str(tmp_path / "algcheck")
+@pytest.fixture(scope="module")
+def algcheck(tmp_path_factory):
+    exe = str(tmp_path_factory.mktemp("alg") / "algcheck")
     subprocess.run(["g++", "-O1", "-std=c++17", os.path.join(HERE, "algebra_host_check.cpp"),
-                    os.path.join(REPO, "oracle", "bssn_oracle_algebra.c"),
+                    "-x", "c", os.path.join(REPO, "oracle", "bssn_oracle_algebra.c"),
+                    os.path.join(REPO, "oracle", "bssn_oracle_constraints.c"), "-x", "none",
                     "-I", os.path.join(REPO, "sympygr_b200", "csrc", "generated"),
                     "-I", os.path.join(REPO, "oracle"), "-o", exe, "-lm"], check=True)
-    out = subprocess.run([exe, "3000"], capture_output=True, text=True, check=True).stdout
+    return exe
+
+
+def test_staged_device_algebra_matches_oracle(algcheck):
+    out = subprocess.run([algcheck, "3000"], capture_output=True, text=True, check=True).stdout
     rel = np.array([float(l.split()[1]) for l in out.strip().splitlines()])
     assert rel.shape == (24,)
+    assert rel.max() < 1e-13, rel
+
+
+def test_staged_constraint_algebra_matches_oracle(algcheck):
+    """The staged device constraint template (ham, mom0..2) against the oracle's flat
+    C constraints, which tests/test_oracle.py pins to the reference's own
+    physical_constraints."""
+    out = subprocess.run([algcheck, "3000", "con"], capture_output=True, text=True,
+                         check=True).stdout
+    rel = np.array([float(l.split()[1]) for l in out.strip().splitlines()])
+    assert rel.shape == (4,)
     assert rel.max() < 1e-13, rel

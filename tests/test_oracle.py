@@ -122,3 +122,54 @@ def test_stencils_exact_on_polynomials(oracle_lib, axis):
         getattr(lib, fns[2])(out.ctypes.data_as(ctypes.c_void_p), f.ctypes.data_as(ctypes.c_void_p),
                              ctypes.c_double(0.1), sz, ctypes.c_uint(0))
         assert np.abs(out[inner]).max() < 1e-9
+
+
+# ---- Hamiltonian and momentum constraints ----------------------------------------
+
+@pytest.mark.parametrize("case", ["con_fake_13_b00", "con_fake_17_b2a"])
+def test_oracle_constraints_match_reference_golden(golden_dir, oracle_lib, case):
+    """The C restatement of the constraints against the reference's own
+    physical_constraints (bssn/CodeGen/physcon.cpp:12) on fake_initial_data."""
+    g = np.load(os.path.join(golden_dir, case + ".npz"))
+    u, blk = po.fake_block(int(g["n"]), tuple(g["pmin"]), float(g["h"]), int(g["bflag"]))
+    assert _sha(u) == str(g["input_sha"])
+    c = po.interior(po.oracle_constraints(u, blk), blk)
+    mx, _ = po.rel_errors(c, g["con_interior"])
+    assert mx.max() < TOL, mx
+
+
+def test_oracle_constraints_match_reference_golden_bl(golden_dir, oracle_lib):
+    g = np.load(os.path.join(golden_dir, "con_bl_70.npz"))
+    u, blk = wl.brill_lindquist(70, 8.0, 1.0)
+    assert _sha(u) == str(g["input_sha"])
+    c = po.interior(po.oracle_constraints(u, blk), blk)
+    scale = np.maximum(g["checksums"][:, 2], 1e-300)[:, None]  # momentum is exactly 0 here
+    assert (np.abs(c[:, g["sample_index"]] - g["sample_con"]) / scale).max() < TOL
+    assert np.allclose(np.abs(c).max(axis=1), g["checksums"][:, 2], rtol=1e-12, atol=0)
+
+
+@pytest.mark.skipif(not po.have_reference("parity"), reason="reference build not present")
+@pytest.mark.parametrize("n,bflag", [(13, 0x3F), (16, 0x15), (19, 0x2A)])
+def test_oracle_constraints_vs_reference_direct(oracle_lib, n, bflag):
+    u, blk = po.fake_block(n, (-0.4, 0.25, -0.15), 0.06, bflag)
+    a = po.interior(po.oracle_constraints(u, blk), blk)
+    b = po.interior(po.ref_constraints(u, blk), blk)[:4]
+    mx, _ = po.rel_errors(a, b)
+    assert mx.max() < TOL, mx
+
+
+def test_constraints_vanish_for_exact_solution(oracle_lib):
+    """Brill-Lindquist data (conformally flat, K = A = 0, Gt = 0) solve the
+    Hamiltonian and momentum constraints: the discrete residual is truncation error
+    that shrinks at the stencils' order as h -> 0."""
+    res = []
+    for n in (38, 70):
+        u, blk = wl.brill_lindquist(n, 8.0, 1.0)
+        c = po.interior(po.oracle_constraints(u, blk), blk)
+        # away from the puncture, where the fields are smooth on both grids
+        x, y, z = (a.ravel() for a in wl.coords(blk))
+        r = np.sqrt(x ** 2 + y ** 2 + z ** 2)[wl.interior_mask(blk).ravel()]
+        far = (r > 3.0) & (r < 6.0)
+        assert np.all(c[1:] == 0.0)  # momentum: every term carries A, K or grad K
+        res.append(np.abs(c[0, far]).max())
+    assert res[1] < res[0] / 8.0, res

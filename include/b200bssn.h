@@ -119,6 +119,9 @@ typedef struct b200bssn_plan_options {
   uint64_t chunk_points;       /* interior points per kernel pair (scratch size) */
   uint32_t slab_depth;         /* max interior z planes per work unit (default 48) */
   uint32_t deriv_ctas_per_sm;  /* resident derivative CTAs per SM (default: as many as fit) */
+  /* NULL, or one entry per block overriding slab_depth for that block (0: keep
+   * slab_depth); lets a tuner pick the depth per block-size class. */
+  const uint32_t *block_slab_depth;
 } b200bssn_plan_options;
 
 /* b200bssn_plan_create with explicit options (opts may be NULL). */
@@ -173,6 +176,54 @@ int b200bssn_physical_constraints(b200bssn_ctx *ctx, double *const *con, const d
 int b200bssn_constraints_plan_device(b200bssn_plan *plan, double *const *con_dev,
                                      const double *const *u_dev, double *block_norms_dev,
                                      void *stream);
+
+/* ---- NaN/Inf guard ------------------------------------------------------- */
+
+/* Scans the interior points of every block of the plan in `narrays` (1..24)
+ * device arrays indexed like the state.  Returns B200BSSN_ERR_NONFINITE if any
+ * value is NaN or infinite, with *first_bad (if non-NULL) the smallest offending
+ * element index; B200BSSN_OK otherwise (*first_bad = UINT64_MAX).  Ghost points
+ * are not scanned.  Synchronous on `stream` (NULL: the context stream). */
+int b200bssn_check_finite(b200bssn_plan *plan, const double *const *arrays, uint32_t narrays,
+                          uint64_t *first_bad, void *stream);
+
+/* ---- RK4 time stepping ---------------------------------------------------- */
+
+/* Classic 4-stage Runge-Kutta over a plan's blocks (BSSN_RK4_STAGES = 4,
+ * bssn/include/parameters.h:37; the reference repository itself has no
+ * integrator).  The stage update runs in the epilogue of the algebra kernel, in
+ * FP64 in both precisions, so a stage is the plan's two launches per chunk and the
+ * RHS never goes to memory.  The object owns three [24][span] FP64 buffers (the
+ * accumulator and two stage states; span = the element range of the plan's
+ * blocks).  Stage kernels write interior points only; ghost points of the stage
+ * states keep what rk4_init (or the caller) put there, so a caller that exchanges
+ * ghosts between blocks does it between stages, on the arrays rk4_stage_state
+ * names.  Blocks with all six faces flagged (bflag 0x3F) never read ghosts. */
+typedef struct b200bssn_rk4 b200bssn_rk4;
+
+int b200bssn_rk4_create(b200bssn_plan *plan, b200bssn_rk4 **rk);
+int b200bssn_rk4_destroy(b200bssn_rk4 *rk);
+/* Copies u_dev's span (ghosts included) into both stage states.  Asynchronous. */
+int b200bssn_rk4_init(b200bssn_rk4 *rk, const double *const *u_dev, void *stream);
+/* Device arrays (24) holding the state that stage `stage` (0..3) reads; stage 0
+ * reads the caller's u and reports NULL pointers. */
+int b200bssn_rk4_stage_state(b200bssn_rk4 *rk, uint32_t stage, double **state);
+/* One stage (0..3) of the step u_dev(t) -> u_dev(t + dt); the last stage updates
+ * u_dev in place.  Asynchronous on `stream` (NULL: the context stream). */
+int b200bssn_rk4_stage(b200bssn_rk4 *rk, uint32_t stage, double *const *u_dev, double dt,
+                       const b200bssn_params *prm, void *stream);
+/* The four stages back to back. */
+int b200bssn_rk4_step(b200bssn_rk4 *rk, double *const *u_dev, double dt,
+                      const b200bssn_params *prm, void *stream);
+/* Captures `steps` (1..1000) full steps for fixed u_dev, dt and prm into a CUDA
+ * graph owned by `rk` (replacing any earlier one); the capture itself runs nothing.
+ * Synchronises the context stream first. */
+int b200bssn_rk4_graph_capture(b200bssn_rk4 *rk, double *const *u_dev, double dt,
+                               const b200bssn_params *prm, uint32_t steps);
+/* Launches the captured graph on `stream` (NULL: the context stream). */
+int b200bssn_rk4_graph_launch(b200bssn_rk4 *rk, void *stream);
+/* Steps in the captured graph (0: none). */
+uint32_t b200bssn_rk4_graph_steps(const b200bssn_rk4 *rk);
 
 /* ---- allocation-free variant --------------------------------------------- */
 

@@ -127,6 +127,54 @@ def oracle_constraints(u, blk, con=None):
     return con
 
 
+def interior_elements(blocks, n_elems):
+    """Boolean mask over element indices: True at every block's interior points."""
+    m = np.zeros(n_elems, dtype=bool)
+    for b in blocks:
+        nx, ny, nz = b.sz
+        idx = np.arange(b.npad).reshape(nz, ny, nx)[3:-3, 3:-3, 3:-3].ravel()
+        m[b.offset + idx] = True
+    return m
+
+
+class OracleRK4:
+    """Classic RK4 over a block list with the oracle's right-hand side: the time
+    stepping the device integrator implements (stage states seeded from the state
+    at ``init`` and updated at interior points only; the state's ghost points are
+    never written).  u is [24, n_elems] float64 and is advanced in place."""
+
+    def __init__(self, blocks, n_elems, prm=None):
+        self.blocks = list(blocks)
+        self.prm = prm or params()
+        self.mask = interior_elements(self.blocks, n_elems)
+        self.sa = self.sb = None
+
+    def init(self, u):
+        self.sa = u.copy()
+        self.sb = u.copy()
+
+    def _rhs(self, state):
+        r = np.zeros_like(state)
+        for b in self.blocks:
+            oracle_rhs(state, b, self.prm, rhs=r)
+        return r[:, self.mask]
+
+    def step(self, u, dt):
+        m = self.mask
+        un = u[:, m]
+        k = self._rhs(u)
+        acc = (dt / 6.0) * k
+        self.sa[:, m] = un + (dt * 0.5) * k
+        k = self._rhs(self.sa)
+        acc += (dt / 3.0) * k
+        self.sb[:, m] = un + (dt * 0.5) * k
+        k = self._rhs(self.sb)
+        acc += (dt / 3.0) * k
+        self.sa[:, m] = un + dt * k
+        k = self._rhs(self.sa)
+        u[:, m] = un + acc + (dt / 6.0) * k
+
+
 def _ref(flavour):
     lib = _load(REF_PARITY if flavour == "parity" else REF_FAST)
     lib.ref_bssnrhs_blocks_omp.restype = ctypes.c_double
@@ -150,6 +198,19 @@ def ref_rhs(u, blk, prm=None, rhs=None, flavour="parity"):
         rhs = np.zeros_like(u)
     lib.ref_bssnrhs(_ptrs(rhs), _ptrs(u), ctypes.c_uint(blk.offset), _dbl3(blk.pmin),
                     _dbl3(blk.pmax), _uint3(blk.sz), ctypes.c_uint(blk.bflag))
+    return rhs
+
+
+def ref_rhs_sep(u, blk, prm=None, rhs=None, flavour="parity"):
+    """The reference's staged bssnrhs_sep (bssn/src/rhs.cpp:392) on one block."""
+    lib = _ref(flavour)
+    prm = prm or params()
+    ref_set_params(lib, prm)
+    u = np.ascontiguousarray(u, dtype=np.float64)
+    if rhs is None:
+        rhs = np.zeros_like(u)
+    lib.ref_bssnrhs_sep(_ptrs(rhs), _ptrs(u), ctypes.c_uint(blk.offset), _dbl3(blk.pmin),
+                        _dbl3(blk.pmax), _uint3(blk.sz), ctypes.c_uint(blk.bflag))
     return rhs
 
 

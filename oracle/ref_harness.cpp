@@ -36,6 +36,14 @@ void ref_bssnrhs(double** rhs, const double** u, unsigned int offset, const doub
   bssnrhs(rhs, u, offset, pmin, pmax, sz, bflag);
 }
 
+// The reference's staged variant (bssn/src/rhs.cpp:392-825, selected by
+// BSSN_RHS_STAGED_COMP in bssnRHS): the same right-hand side evaluated one
+// equation group at a time.
+void ref_bssnrhs_sep(double** rhs, const double** u, unsigned int offset, const double* pmin,
+                     const double* pmax, const unsigned int* sz, unsigned int bflag) {
+  bssnrhs_sep(rhs, u, offset, pmin, pmax, sz, bflag);
+}
+
 // Block list through the reference's block-parallel OpenMP loop
 // (bssn/cuda_gr/src/gpuBSSNExample.cpp:267-299: `#pragma omp parallel for` over
 // blocks, one bssnrhs per block). Returns the wall-clock seconds of the loop.

@@ -12,11 +12,11 @@ of the reference's entry point:
 which follows ``bssnrhs(uzipVarsRHS, uZipVars, offset, ptmin, ptmax, sz, bflag)``
 (bssn/include/rhs.h:33-36).
 """
-from .capi import (FP64, GHOSTS_PRESERVE, GHOSTS_ZERO, MIXED, B200BssnError, Context, Params,
+from .capi import (FP64, GHOSTS_PRESERVE, GHOSTS_ZERO, MIXED, RK4, B200BssnError, Context, Params,
                    Plan, load)
 from .workloads import Block
 
-__all__ = ["Context", "Plan", "Params", "Block", "B200BssnError", "FP64", "MIXED",
+__all__ = ["Context", "Plan", "RK4", "Params", "Block", "B200BssnError", "FP64", "MIXED",
            "GHOSTS_PRESERVE", "GHOSTS_ZERO", "bssnrhs", "load"]
 
 

@@ -1,0 +1,128 @@
+"""Autotuner: per block-size class, the plan knobs that evaluate the right-hand side
+fastest on this GPU.
+
+For each padded size class of the two-puncture batch (13, 21, 37, 69, 135; the
+class's block count from the batch, times --scale) it builds a plan of that class
+alone and times one evaluation (CUDA events, device-resident inputs larger than L2)
+for every candidate of
+
+* slab depth: the z-planes per work unit of the derivative kernel (candidates that
+  cut the interior into the same number of slabs are the same plan, so one per
+  slab count is timed);
+* derivative CTAs per SM (1 or 2 resident persistent CTAs).
+
+It writes the per-class table and choice to JSON.  ``tuned_plan`` builds a plan
+for any block list from such a table: each block gets its class's slab depth
+(b200bssn_plan_options.block_slab_depth); the CTA count, a plan-wide knob, is the
+choice of the class holding the most points.  The run ends with the whole batch
+timed with the default knobs and with the tuned ones.
+
+    python -m sympygr_b200.autotune --precision mixed --json gpurun_out/tune_mixed.json
+"""
+from __future__ import annotations
+
+import argparse
+import json
+
+from . import capi
+from . import workloads as wl
+
+
+def depth_candidates(n: int):
+    """One depth per distinct slab count of an n^3 block (interior n-6 planes)."""
+    planes = n - 6
+    out, seen = [], set()
+    for d in (8, 12, 16, 24, 32, 40, 48, 64, 96, 128, planes):
+        d = min(d, planes)
+        ns = -(-planes // d)
+        if ns not in seen:
+            seen.add(ns)
+            out.append(d)
+    return out
+
+
+def time_plan(plan, rhs, u, prm, reps: int = 5, warmup: int = 2) -> float:
+    """Milliseconds per evaluation (CUDA events on the context stream)."""
+    import torch
+
+    stream = torch.cuda.ExternalStream(plan.ctx.stream)
+    for _ in range(warmup):
+        plan.rhs_device(rhs, u, prm)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        plan.rhs_device(rhs, u, prm)
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def tuned_plan(ctx, blocks, precision, table, chunk_points: int = 0):
+    """A plan whose blocks use their size class's tuned slab depth."""
+    choice = {int(k): v for k, v in table["choice"].items()}
+    depths = [choice.get(b.sz[2], {}).get("slab_depth", 0) for b in blocks]
+    return capi.Plan(ctx, blocks, precision, chunk_points, deriv_ctas_per_sm=table["deriv_ctas_per_sm"],
+                     block_slab_depth=depths)
+
+
+def main(argv=None):
+    import torch
+
+    ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--scale", type=float, default=1.0)
+    ap.add_argument("--reps", type=int, default=5)
+    ap.add_argument("--json", default="")
+    args = ap.parse_args(argv)
+    prec = capi.MIXED if args.precision == "mixed" else capi.FP64
+    prm = capi.Params.make(ko_sigma=0.4, precision=prec)
+    ctx = capi.Context(0)
+    counts = tuple(max(1, int(round(c * args.scale))) for c in wl.BATCH_COUNTS)
+    table = {"precision": args.precision, "classes": {}, "choice": {}}
+    best_points = (0, 0)
+    for n, c in zip(wl.BATCH_SIZES, counts):
+        u, blocks = wl.two_puncture_batch_torch((n,), (c,), seed=1, device="cuda")
+        rhs = torch.zeros_like(u)
+        pts = sum(b.ninterior for b in blocks)
+        rows = []
+        for d in depth_candidates(n):
+            for ctas in (1, 2):
+                plan = capi.Plan(ctx, blocks, prec, slab_depth=d, deriv_ctas_per_sm=ctas)
+                ms = time_plan(plan, list(rhs), list(u), prm, args.reps)
+                plan.close()
+                rows.append({"slab_depth": d, "deriv_ctas_per_sm": ctas, "ms": ms,
+                             "mpts_per_s": pts / ms / 1e3})
+                print(json.dumps({"class": n, **rows[-1]}), flush=True)
+        best = max(rows, key=lambda r: r["mpts_per_s"])
+        table["classes"][str(n)] = {"blocks": c, "points": pts, "runs": rows}
+        table["choice"][str(n)] = {"slab_depth": best["slab_depth"],
+                                   "deriv_ctas_per_sm": best["deriv_ctas_per_sm"],
+                                   "mpts_per_s": best["mpts_per_s"]}
+        if pts > best_points[0]:
+            best_points = (pts, best["deriv_ctas_per_sm"])
+        del u, rhs
+        torch.cuda.empty_cache()
+    table["deriv_ctas_per_sm"] = best_points[1]
+    # the whole batch: default knobs against the tuned table
+    u, blocks = wl.two_puncture_batch_torch(wl.BATCH_SIZES, counts, seed=0, device="cuda")
+    rhs = torch.zeros_like(u)
+    pts = sum(b.ninterior for b in blocks)
+    plan = capi.Plan(ctx, blocks, prec)
+    ms_default = time_plan(plan, list(rhs), list(u), prm, args.reps)
+    plan.close()
+    plan = tuned_plan(ctx, blocks, prec, table)
+    ms_tuned = time_plan(plan, list(rhs), list(u), prm, args.reps)
+    plan.close()
+    table["batch"] = {"points": pts, "default_mpts_per_s": pts / ms_default / 1e3,
+                      "tuned_mpts_per_s": pts / ms_tuned / 1e3}
+    print(json.dumps({"choice": table["choice"], "batch": table["batch"],
+                      "deriv_ctas_per_sm": table["deriv_ctas_per_sm"]}), flush=True)
+    if args.json:
+        with open(args.json, "w") as f:
+            json.dump(table, f, indent=1)
+    ctx.close()
+    return table
+
+
+if __name__ == "__main__":
+    main()

@@ -91,6 +91,7 @@ class PlanOptions(ctypes.Structure):
         ("chunk_points", ctypes.c_uint64),
         ("slab_depth", ctypes.c_uint32),
         ("deriv_ctas_per_sm", ctypes.c_uint32),
+        ("block_slab_depth", ctypes.POINTER(ctypes.c_uint32)),
     ]
 
 
@@ -125,6 +126,19 @@ SIGNATURES = [
      [_P, _P, _P, ctypes.c_uint32, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
       ctypes.POINTER(ctypes.c_uint32), ctypes.c_uint32, ctypes.c_uint32]),
     ("b200bssn_constraints_plan_device", ctypes.c_int, [_P, _P, _P, _P, _P]),
+    ("b200bssn_check_finite", ctypes.c_int, [_P, _P, ctypes.c_uint32,
+                                             ctypes.POINTER(ctypes.c_uint64), _P]),
+    ("b200bssn_rk4_create", ctypes.c_int, [_P, ctypes.POINTER(_P)]),
+    ("b200bssn_rk4_destroy", ctypes.c_int, [_P]),
+    ("b200bssn_rk4_init", ctypes.c_int, [_P, _P, _P]),
+    ("b200bssn_rk4_stage_state", ctypes.c_int, [_P, ctypes.c_uint32, _P]),
+    ("b200bssn_rk4_stage", ctypes.c_int, [_P, ctypes.c_uint32, _P, ctypes.c_double,
+                                          ctypes.POINTER(Params), _P]),
+    ("b200bssn_rk4_step", ctypes.c_int, [_P, _P, ctypes.c_double, ctypes.POINTER(Params), _P]),
+    ("b200bssn_rk4_graph_capture", ctypes.c_int, [_P, _P, ctypes.c_double, ctypes.POINTER(Params),
+                                                  ctypes.c_uint32]),
+    ("b200bssn_rk4_graph_launch", ctypes.c_int, [_P, _P]),
+    ("b200bssn_rk4_graph_steps", ctypes.c_uint32, [_P]),
     ("b200bssn_rhs_noalloc", ctypes.c_int, [_P, _P, ctypes.POINTER(BlockC), ctypes.POINTER(Params), _P]),
     ("b200bssn_debug_block_scratch", ctypes.c_int, [_P, _P, ctypes.c_uint64]),
     ("b200bssn_fma_peak", ctypes.c_int, [ctypes.c_int, ctypes.c_uint32, ctypes.POINTER(ctypes.c_double)]),
@@ -266,7 +280,8 @@ class Plan:
     """``b200bssn_plan``: descriptors and scratch for a fixed block list."""
 
     def __init__(self, ctx: Context, blocks: Sequence[Block], precision: int = FP64,
-                 chunk_points: int = 0, slab_depth: int = 0, deriv_ctas_per_sm: int = 0):
+                 chunk_points: int = 0, slab_depth: int = 0, deriv_ctas_per_sm: int = 0,
+                 block_slab_depth: Sequence[int] | None = None):
         lib = load()
         arr = (BlockC * len(blocks))()
         for i, b in enumerate(blocks):
@@ -278,6 +293,11 @@ class Plan:
             arr[i].bflag = b.bflag
         h = ctypes.c_void_p()
         opts = PlanOptions(chunk_points, slab_depth, deriv_ctas_per_sm)
+        if block_slab_depth is not None:
+            if len(block_slab_depth) != len(blocks):
+                raise ValueError("block_slab_depth needs one entry per block")
+            depths = (ctypes.c_uint32 * len(blocks))(*[int(d) for d in block_slab_depth])
+            opts.block_slab_depth = depths
         _check(lib.b200bssn_plan_create_ex(ctx.handle, arr, len(blocks), precision,
                                            ctypes.byref(opts), ctypes.byref(h)),
                "b200bssn_plan_create_ex", ctx)
@@ -317,6 +337,19 @@ class Plan:
                                                        ctypes.c_void_p(stream or None)),
                "b200bssn_constraints_plan_device", self.ctx)
 
+    def check_finite(self, arrays, stream: int = 0):
+        """NaN/Inf guard over the interior points of the plan's blocks in the given
+        device arrays (1..24).  Returns None if all finite, else the smallest
+        offending element index."""
+        n = len(arrays)
+        bad = ctypes.c_uint64()
+        rc = load().b200bssn_check_finite(self.handle, _ptr_table(arrays, n), n, ctypes.byref(bad),
+                                          ctypes.c_void_p(stream or None))
+        if rc == -6:
+            return int(bad.value)
+        _check(rc, "b200bssn_check_finite", self.ctx)
+        return None
+
     def profile(self, rhs, u, params: Params):
         """One evaluation with per-launch events: (derivative ms, algebra ms)."""
         d, a = ctypes.c_double(), ctypes.c_double()
@@ -334,6 +367,66 @@ class Plan:
     def close(self):
         if self.handle:
             load().b200bssn_plan_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class RK4:
+    """``b200bssn_rk4``: classic RK4 over a plan's blocks, stage update fused into the
+    algebra kernel.  `u` is the list of 24 device arrays the state lives in; the
+    object keeps pointers to them for graph capture, so keep them alive."""
+
+    def __init__(self, plan: Plan):
+        lib = load()
+        h = ctypes.c_void_p()
+        _check(lib.b200bssn_rk4_create(plan.handle, ctypes.byref(h)), "b200bssn_rk4_create", plan.ctx)
+        self.plan = plan
+        self.handle = h
+
+    def init(self, u, stream: int = 0):
+        """Copy the state (ghosts included) into both stage states."""
+        _check(load().b200bssn_rk4_init(self.handle, _ptr_table(u), ctypes.c_void_p(stream or None)),
+               "b200bssn_rk4_init", self.plan.ctx)
+
+    def stage_state(self, stage: int):
+        """Device pointers (24 ints; 0 for stage 0) of the state stage `stage` reads."""
+        out = (ctypes.c_void_p * NUM_VARS)()
+        _check(load().b200bssn_rk4_stage_state(self.handle, stage, out), "b200bssn_rk4_stage_state",
+               self.plan.ctx)
+        return [int(p or 0) for p in out]
+
+    def stage(self, stage: int, u, dt: float, params: Params, stream: int = 0):
+        _check(load().b200bssn_rk4_stage(self.handle, stage, _ptr_table(u), float(dt),
+                                         ctypes.byref(params), ctypes.c_void_p(stream or None)),
+               "b200bssn_rk4_stage", self.plan.ctx)
+
+    def step(self, u, dt: float, params: Params, stream: int = 0):
+        _check(load().b200bssn_rk4_step(self.handle, _ptr_table(u), float(dt), ctypes.byref(params),
+                                        ctypes.c_void_p(stream or None)),
+               "b200bssn_rk4_step", self.plan.ctx)
+
+    def capture(self, u, dt: float, params: Params, steps: int = 1):
+        """Capture `steps` full steps into a CUDA graph (replay with ``launch``)."""
+        _check(load().b200bssn_rk4_graph_capture(self.handle, _ptr_table(u), float(dt),
+                                                 ctypes.byref(params), int(steps)),
+               "b200bssn_rk4_graph_capture", self.plan.ctx)
+
+    def launch(self, stream: int = 0):
+        _check(load().b200bssn_rk4_graph_launch(self.handle, ctypes.c_void_p(stream or None)),
+               "b200bssn_rk4_graph_launch", self.plan.ctx)
+
+    @property
+    def graph_steps(self) -> int:
+        return int(load().b200bssn_rk4_graph_steps(self.handle))
+
+    def close(self):
+        if self.handle:
+            load().b200bssn_rk4_destroy(self.handle)
             self.handle = None
 
     def __del__(self):

@@ -10,94 +10,38 @@
 
 #include "b200bssn.h"
 #include "constraint_kernels.cuh"
+#include "plan_internal.h"
 #include "rhs_kernels.cuh"
 
 using namespace b200bssn;
+using b200bssn::host::fail_cuda;
+using b200bssn::host::launch_plan;
+using b200bssn::host::params_ok;
 
-struct b200bssn_ctx {
-  int device = 0;
-  cudaStream_t stream = nullptr;
-  // derivative and algebra streams of the chunk pipeline (see launch_plan), and
-  // the upload / download streams of the pipelined host path
-  cudaStream_t s_deriv = nullptr, s_alg = nullptr, s_h2d = nullptr, s_d2h = nullptr;
-  std::string last_error;
-  // single-block drop-in path
-  double* blk_u = nullptr;    // [24][npad]
-  double* blk_rhs = nullptr;  // [24][npad]
-  size_t blk_cap = 0;         // npad capacity
-  b200bssn_plan* blk_plan = nullptr;
-  uint32_t blk_sz[3] = {0, 0, 0};
-  uint32_t blk_precision = 0xffffffffu;
-};
-
-struct ChunkRec {
-  int32_t tile_begin, tile_count;
-  int32_t range_begin, range_count;
-  int64_t points;
-};
-
-struct b200bssn_plan {
-  b200bssn_ctx* ctx = nullptr;
-  uint32_t precision = 0;
-  std::vector<BlockDev> blocks;
-  std::vector<UnitDev> units;
-  std::vector<TileDev> tiles;
-  std::vector<RangeDev> ranges;
-  std::vector<ChunkRec> chunks;
-  uint64_t points = 0;
-  int64_t cap = 0;
-  uint64_t span_lo = 0, span_hi = 0;  // element range touched in the variable arrays
-  // device
-  void* desc = nullptr;  // blocks | units | tiles | ranges
-  BlockDev* d_blocks = nullptr;
-  UnitDev* d_units = nullptr;
-  TileDev* d_tiles = nullptr;
-  RangeDev* d_ranges = nullptr;
-  // derivative scratch: two buffers when the plan has more than one chunk, so the
-  // derivative kernel of chunk c+1 can run while the algebra kernel of chunk c reads
-  void* dscr[2] = {nullptr, nullptr};
-  double* koscr[2] = {nullptr, nullptr};
-  std::vector<cudaEvent_t> ev_deriv, ev_alg;  // per chunk: derivative / algebra done
-  cudaEvent_t ev_fork = nullptr;
-  int* d_counters = nullptr;  // per chunk: work counter of the derivative kernel
-  // pipelined host path: element ranges [part[c], part[c+1]) partition the span, one
-  // per chunk, when chunks hold whole blocks in increasing offset order
-  bool host_pipeline = false;
-  std::vector<uint64_t> part;
-  std::vector<cudaEvent_t> ev_in;  // per chunk: upload done
-  int deriv_grid = 0;         // resident CTAs of the persistent derivative kernel
-  // host-batch staging (allocated on first host call)
-  double* st_u = nullptr;
-  double* st_rhs = nullptr;
-  uint64_t st_len = 0;
-};
-
-namespace {
-
-int fail_cuda(b200bssn_ctx* ctx, cudaError_t e, const char* what) {
+int b200bssn::host::fail_cuda(b200bssn_ctx* ctx, cudaError_t e, const char* what) {
   if (ctx) {
     ctx->last_error = std::string(what) + ": " + cudaGetErrorString(e);
   }
   return e == cudaErrorMemoryAllocation ? B200BSSN_ERR_OUT_OF_MEMORY : B200BSSN_ERR_CUDA;
 }
 
-#define CK(ctx, call)                                   \
-  do {                                                  \
-    cudaError_t e_ = (call);                            \
-    if (e_ != cudaSuccess) return fail_cuda(ctx, e_, #call); \
-  } while (0)
+bool b200bssn::host::params_ok(const b200bssn_params* p) {
+  return p && (p->precision == B200BSSN_FP64 || p->precision == B200BSSN_MIXED) &&
+         (p->ghost_policy == B200BSSN_GHOSTS_PRESERVE || p->ghost_policy == B200BSSN_GHOSTS_ZERO);
+}
+
+#define CK B200BSSN_CK
+
+namespace {
 
 constexpr int64_t kDefaultChunkPoints = int64_t(1) << 23;
 // scratch slots are addressed with 32-bit offsets: kNumDerivs * cap < 2^31
 constexpr int64_t kMaxChunkPoints = (int64_t(1) << 31) / (kNumDerivs + 1) - 1;
 
-bool params_ok(const b200bssn_params* p) {
-  return p && (p->precision == B200BSSN_FP64 || p->precision == B200BSSN_MIXED) &&
-         (p->ghost_policy == B200BSSN_GHOSTS_PRESERVE || p->ghost_policy == B200BSSN_GHOSTS_ZERO);
-}
-
 void make_args(const b200bssn_plan* P, double* const* rhs, const double* const* u,
                const b200bssn_params* prm, DerivArgs& da, AlgebraArgs& aa) {
+  std::memset(&da, 0, sizeof(da));
+  std::memset(&aa, 0, sizeof(aa));  // aa.rk.mode = RK_NONE: store the RHS
   for (int v = 0; v < kNumVars; ++v) {
     da.u[v] = u[v];
     aa.u[v] = u[v];
@@ -179,14 +123,18 @@ int enqueue_chunk(b200bssn_plan* P, DerivArgs da, AlgebraArgs aa, size_t ci, int
 // `s` in order, with events ev[4c+0..3] around chunk c's two kernels.
 //
 // With `ca` non-null the second kernel of every chunk is the constraint kernel
-// (`rhs` and `prm` are then only used to fill the unused algebra arguments).
-int launch_plan(b200bssn_plan* P, double* const* rhs, const double* const* u,
-                const b200bssn_params* prm, cudaStream_t s, cudaEvent_t* ev = nullptr,
-                const ConstraintArgs* ca = nullptr) {
+// (`rhs` and `prm` are then only used to fill the unused algebra arguments); with
+// `rk` non-null the algebra kernel applies that RK4 stage update (`rhs` unused).
+}  // namespace
+
+int b200bssn::host::launch_plan(b200bssn_plan* P, double* const* rhs, const double* const* u,
+                                const b200bssn_params* prm, cudaStream_t s, cudaEvent_t* ev,
+                                const ConstraintArgs* ca, const RkStage* rk) {
   b200bssn_ctx* ctx = P->ctx;
   DerivArgs da;
   AlgebraArgs aa;
   make_args(P, rhs, u, prm, da, aa);
+  if (rk) aa.rk = *rk;
   const size_t nch = P->chunks.size();
   const bool pipelined = ev == nullptr && nch > 1;
   cudaStream_t s1 = pipelined ? ctx->s_deriv : s, s2 = pipelined ? ctx->s_alg : s;
@@ -204,6 +152,8 @@ int launch_plan(b200bssn_plan* P, double* const* rhs, const double* const* u,
   if (pipelined) CK(ctx, cudaStreamWaitEvent(s, P->ev_alg[nch - 1], 0));
   return B200BSSN_OK;
 }
+
+namespace {
 
 int set_kernel_attributes(b200bssn_ctx* ctx) {
   CK(ctx, cudaFuncSetAttribute(bssn_derivs_kernel<double>,
@@ -352,9 +302,11 @@ int b200bssn_plan_create_ex(b200bssn_ctx* ctx, const b200bssn_block* blocks, uin
     P->span_lo = std::min<uint64_t>(P->span_lo, in.offset);
     P->span_hi = std::max<uint64_t>(P->span_hi, in.offset + npad);
     const int64_t I0 = in.sz[0] - 6, I1 = in.sz[1] - 6, I2 = in.sz[2] - 6;
-    // z-slabs of nearly equal depth (<= slab_depth planes): the derivative kernel
+    // z-slabs of nearly equal depth (<= depth planes): the derivative kernel
     // streams each slab plus 4 halo planes on each side
-    const int64_t nslab = (I2 + slab_depth - 1) / slab_depth;
+    const int64_t depth = (o.block_slab_depth && o.block_slab_depth[b])
+                              ? (int64_t)o.block_slab_depth[b] : slab_depth;
+    const int64_t nslab = (I2 + depth - 1) / depth;
     if ((uint64_t)I0 * I1 * ((I2 + nslab - 1) / nslab) > (uint64_t)INT32_MAX) {
       delete P;
       return B200BSSN_ERR_INVALID_ARGUMENT;
@@ -532,6 +484,7 @@ int b200bssn_plan_destroy(b200bssn_plan* P) {
     if (e) cudaEventDestroy(e);
   if (P->ev_fork) cudaEventDestroy(P->ev_fork);
   cudaFree(P->d_counters);
+  cudaFree(P->d_guard);
   cudaFree(P->st_u);
   cudaFree(P->st_rhs);
   delete P;

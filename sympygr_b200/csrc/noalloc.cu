@@ -24,6 +24,8 @@
 //    with that device current; make that first call before any stream capture.
 #include <cuda_runtime.h>
 
+#include <cstring>
+
 #include <mutex>
 
 #include "b200bssn.h"
@@ -177,6 +179,8 @@ extern "C" int b200bssn_rhs_noalloc(double* const* rhs_dev, const double* const*
 
   DerivArgs da;
   AlgebraArgs aa;
+  std::memset(&da, 0, sizeof(da));
+  std::memset(&aa, 0, sizeof(aa));  // aa.rk.mode = RK_NONE: store the RHS
   for (int v = 0; v < kNumVars; ++v) {
     da.u[v] = u_dev[v];
     aa.u[v] = u_dev[v];

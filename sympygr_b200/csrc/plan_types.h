@@ -48,4 +48,23 @@ struct RangeDev {
   int32_t count;     // <= kAlgebraThreads
 };
 
+// Classic RK4 stage update fused into the algebra kernel's epilogue.  With k the
+// right-hand side at a point (in FP64, KO included) and u^n the state at the start
+// of the step:
+//   RK_FIRST   acc  = w k          next = u^n + c k      (stage 1)
+//   RK_MIDDLE  acc += w k          next = u^n + c k      (stages 2, 3)
+//   RK_LAST    u^n  = u^n + acc + w k                     (stage 4)
+// with w = dt/6, dt/3, dt/3, dt/6 and c = dt/2, dt/2, dt.  Every array is read and
+// written at the thread's own point only, so the kernel's inputs (the stage state
+// `u`, read at the point and by the derivative kernel) never alias its outputs.
+enum RkMode : int32_t { RK_NONE = 0, RK_FIRST = 1, RK_MIDDLE = 2, RK_LAST = 3 };
+
+struct RkStage {
+  int32_t mode;
+  double w, c;
+  double* acc[kNumVars];
+  double* next[kNumVars];
+  double* base[kNumVars];  // u^n: read in every stage, written in RK_LAST
+};
+
 }  // namespace b200bssn

@@ -10,7 +10,9 @@
 //  bssn_algebra_kernel  one thread per interior point: the generated BSSN algebra
 //                       (or, on a flagged face plane, the Sommerfeld value of
 //                       bssn/src/rhs.cpp:833-977), plus sigma times the KO sum
-//                       (bssn/src/rhs.cpp:332-369), written to the RHS arrays.
+//                       (bssn/src/rhs.cpp:332-369), written to the RHS arrays --
+//                       or, in an RK4 stage, folded straight into the stage update
+//                       (see RkStage) so the RHS never goes to memory.
 #pragma once
 #include <stdint.h>
 
@@ -491,6 +493,7 @@ constexpr size_t kDerivSmemBytes = 0;  // all shared memory is static
 struct AlgebraArgs {
   const double* u[kNumVars];
   double* rhs[kNumVars];
+  RkStage rk;
   const BlockDev* blocks;
   const UnitDev* units;
   const RangeDev* ranges;
@@ -522,6 +525,21 @@ struct PointIn {
   }
 };
 
+// Stores the right-hand side k of variable v at element pp: to the RHS arrays, or
+// through the RK4 stage update.
+// Any mode other than the three stage modes stores the RHS.
+__device__ __forceinline__ void store_rhs(const AlgebraArgs& a, int v, int64_t pp, double k) {
+  const RkStage& rk = a.rk;
+  if (rk.mode == RK_LAST) {
+    rk.base[v][pp] = rk.base[v][pp] + rk.acc[v][pp] + rk.w * k;
+  } else if (rk.mode == RK_FIRST || rk.mode == RK_MIDDLE) {
+    rk.acc[v][pp] = rk.mode == RK_FIRST ? rk.w * k : rk.acc[v][pp] + rk.w * k;
+    rk.next[v][pp] = __ldg(rk.base[v] + pp) + rk.c * k;
+  } else {
+    a.rhs[v][pp] = k;
+  }
+}
+
 struct PointSink {
   const AlgebraArgs* a;
   int64_t pp;
@@ -529,7 +547,7 @@ struct PointSink {
   template <typename RT>
   __device__ __forceinline__ void put(int v, RT val) {
     // rhs += sigma * (ko_x + ko_y + ko_z), rounded as rhs.cpp:332-369 rounds it
-    a->rhs[v][pp] = __dadd_rn((double)val, __dmul_rn(a->ko_sigma, __ldg(a->koscr + v * a->cap + lp)));
+    store_rhs(*a, v, pp, __dadd_rn((double)val, __dmul_rn(a->ko_sigma, __ldg(a->koscr + v * a->cap + lp))));
   }
 };
 
@@ -572,7 +590,7 @@ bssn_algebra_kernel(const __grid_constant__ AlgebraArgs a) {
       t = __dadd_rn(t, __dmul_rn(z, dzf));
       t = __dadd_rn(t, __dmul_rn(bc_falloff(v), __dsub_rn(f, bc_asymptotic(v))));
       const double val = __dmul_rn(-inv_r, t);
-      a.rhs[v][pp] = __dadd_rn(val, __dmul_rn(a.ko_sigma, __ldg(a.koscr + v * a.cap + lp)));
+      store_rhs(a, v, pp, __dadd_rn(val, __dmul_rn(a.ko_sigma, __ldg(a.koscr + v * a.cap + lp))));
     }
     return;
   }

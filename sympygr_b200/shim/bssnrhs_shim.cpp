@@ -12,6 +12,21 @@
 // library context, so the reference's OpenMP block loop
 // (bssn/cuda_gr/src/gpuBSSNExample.cpp:267-299) keeps working unchanged.
 //
+// The staged variant bssnrhs_sep (bssn/include/rhs.h:39, bssn/src/rhs.cpp:392-825),
+// which bssnRHS calls instead when built with BSSN_RHS_STAGED_COMP, computes the same
+// right-hand side one equation group at a time (it agrees with bssnrhs to ~2e-15);
+// it is defined here too, on the same GPU path.
+//
+// It also replaces the reference's constraint evaluator
+//
+//   void physical_constraints(double **uZipConVars, const double **uZipVars,
+//                             const unsigned int &offset, const double *pmin,
+//                             const double *pmax, const unsigned int *sz,
+//                             const unsigned int &bflag);   (bssn/CodeGen/physcon.cpp:12-15)
+//
+// writing uZipConVars[C_HAM..C_MOM2] (bssn/include/grDef.h:40) at the interior
+// points; the Psi4 arrays (C_PSI4_REAL, C_PSI4_IMG) are left untouched.
+//
 // Environment: B200BSSN_DEVICE (CUDA device, default 0), B200BSSN_PRECISION
 // ("fp64" default, or "mixed").  The reference function returns nothing; a
 // failure here throws std::runtime_error with the library's message.
@@ -80,4 +95,22 @@ void bssnrhs(double** uzipVarsRHS, const double** uZipVars, const unsigned int& 
   if (rc != B200BSSN_OK)
     throw std::runtime_error(std::string("bssnrhs: ") + b200bssn_status_string(rc) + " (" +
                              b200bssn_last_error(ctx) + ")");
+}
+
+void bssnrhs_sep(double** uzipVarsRHS, const double** uZipVars, const unsigned int& offset,
+                 const double* ptmin, const double* ptmax, const unsigned int* sz,
+                 const unsigned int& bflag) {
+  bssnrhs(uzipVarsRHS, uZipVars, offset, ptmin, ptmax, sz, bflag);
+}
+
+void physical_constraints(double** uZipConVars, const double** uZipVars, const unsigned int& offset,
+                          const double* pmin, const double* pmax, const unsigned int* sz,
+                          const unsigned int& bflag) {
+  b200bssn_ctx* ctx = thread_ctx();
+  const uint32_t usz[3] = {sz[0], sz[1], sz[2]};
+  const int rc = b200bssn_physical_constraints(ctx, uZipConVars, uZipVars, offset, pmin, pmax, usz,
+                                               bflag, precision_from_env());
+  if (rc != B200BSSN_OK)
+    throw std::runtime_error(std::string("physical_constraints: ") + b200bssn_status_string(rc) +
+                             " (" + b200bssn_last_error(ctx) + ")");
 }

@@ -1,7 +1,9 @@
-// Test driver for the bssnrhs shim: stands in for the host code (it defines the
-// bssn:: globals, as the host's parameters.cpp would), fills one block from a raw
-// input file, calls bssnrhs with the reference's signature, and writes the RHS.
-//   shim_test <in.bin> <out.bin> <n> <pmin> <h> <bflag> <sigma>
+// Test driver for the shim: stands in for the host code (it defines the bssn::
+// globals, as the host's parameters.cpp would), fills one block from a raw input
+// file, calls bssnrhs (or, with an 8th argument "sep", bssnrhs_sep; "con",
+// physical_constraints) with the reference's signature, and writes the 24 RHS (or 6
+// constraint) arrays.
+//   shim_test <in.bin> <out.bin> <n> <pmin> <h> <bflag> <sigma> [sep|con]
 #include <cstdio>
 #include <cstdlib>
 #include <vector>
@@ -9,6 +11,12 @@
 void bssnrhs(double** uzipVarsRHS, const double** uZipVars, const unsigned int& offset,
              const double* ptmin, const double* ptmax, const unsigned int* sz,
              const unsigned int& bflag);
+void physical_constraints(double** uZipConVars, const double** uZipVars, const unsigned int& offset,
+                          const double* pmin, const double* pmax, const unsigned int* sz,
+                          const unsigned int& bflag);
+void bssnrhs_sep(double** uzipVarsRHS, const double** uZipVars, const unsigned int& offset,
+                 const double* ptmin, const double* ptmax, const unsigned int* sz,
+                 const unsigned int& bflag);
 
 namespace bssn {
 unsigned int BSSN_LAMBDA[4] = {1, 1, 1, 1};
@@ -20,13 +28,16 @@ double KO_DISS_SIGMA = 0.01;
 }  // namespace bssn
 
 int main(int argc, char** argv) {
-  if (argc != 8) return 2;
+  if (argc != 8 && argc != 9) return 2;
+  const bool con = argc == 9 && argv[8][0] == 'c';
+  const bool sep = argc == 9 && argv[8][0] == 's';
   const unsigned n = (unsigned)std::atoi(argv[3]);
   const double p0 = std::atof(argv[4]), h = std::atof(argv[5]);
   const unsigned bflag = (unsigned)std::atoi(argv[6]);
   bssn::KO_DISS_SIGMA = std::atof(argv[7]);
   const size_t npad = (size_t)n * n * n;
-  std::vector<double> u(24 * npad), r(24 * npad, 0.0);
+  const int nout = con ? 6 : 24;
+  std::vector<double> u(24 * npad), r(nout * npad, 0.0);
   FILE* f = std::fopen(argv[1], "rb");
   if (!f || std::fread(u.data(), sizeof(double), u.size(), f) != u.size()) return 3;
   std::fclose(f);
@@ -34,13 +45,18 @@ int main(int argc, char** argv) {
   double* rp[24];
   for (int v = 0; v < 24; ++v) {
     up[v] = u.data() + v * npad;
-    rp[v] = r.data() + v * npad;
+    rp[v] = v < nout ? r.data() + v * npad : nullptr;
   }
   const double pmin[3] = {p0, p0, p0}, pmax[3] = {p0 + (n - 1) * h, p0 + (n - 1) * h, p0 + (n - 1) * h};
   const unsigned sz[3] = {n, n, n};
   const unsigned offset = 0;
   try {
-    bssnrhs(rp, up, offset, pmin, pmax, sz, bflag);
+    if (con)
+      physical_constraints(rp, up, offset, pmin, pmax, sz, bflag);
+    else if (sep)
+      bssnrhs_sep(rp, up, offset, pmin, pmax, sz, bflag);
+    else
+      bssnrhs(rp, up, offset, pmin, pmax, sz, bflag);
   } catch (...) {
     return 4;
   }

@@ -45,17 +45,18 @@ def test_every_declared_function_is_exported(lib):
 def test_struct_layouts_match_c(tmp_path):
     src = tmp_path / "layout.c"
     src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "b200bssn.h"\n'
-                   'int main(void){printf("%zu %zu %zu %zu %zu %zu\\n", sizeof(b200bssn_params),'
+                   'int main(void){printf("%zu %zu %zu %zu %zu %zu %zu\\n", sizeof(b200bssn_params),'
                    ' offsetof(b200bssn_params, precision), sizeof(b200bssn_block),'
                    ' offsetof(b200bssn_block, pmin), sizeof(b200bssn_plan_options),'
-                   ' offsetof(b200bssn_plan_options, deriv_ctas_per_sm)); return 0;}\n')
+                   ' offsetof(b200bssn_plan_options, deriv_ctas_per_sm),'
+                   ' offsetof(b200bssn_plan_options, block_slab_depth)); return 0;}\n')
     exe = tmp_path / "layout"
     subprocess.run(["gcc", "-I", os.path.join(REPO, "include"), str(src), "-o", str(exe)], check=True)
     got = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True,
                                           check=True).stdout.split()]
     want = [ctypes.sizeof(capi.Params), capi.Params.precision.offset, ctypes.sizeof(capi.BlockC),
             capi.BlockC.pmin.offset, ctypes.sizeof(capi.PlanOptions),
-            capi.PlanOptions.deriv_ctas_per_sm.offset]
+            capi.PlanOptions.deriv_ctas_per_sm.offset, capi.PlanOptions.block_slab_depth.offset]
     assert got == want
 
 
@@ -91,6 +92,11 @@ def test_shim_exports_the_reference_symbol():
     # void bssnrhs(double**, const double**, const unsigned&, const double*, const double*,
     #              const unsigned*, const unsigned&)   (bssn/include/rhs.h:33-36)
     assert "_Z7bssnrhsPPdPPKdRKjS2_S2_PS4_S5_" in defined
+    # void physical_constraints(double**, const double**, const unsigned&, const double*,
+    #                           const double*, const unsigned*, const unsigned&)
+    #                                                  (bssn/CodeGen/physcon.cpp:12-15)
+    assert "_Z20physical_constraintsPPdPPKdRKjS2_S2_PS4_S5_" in defined
+    assert "_Z11bssnrhs_sepPPdPPKdRKjS2_S2_PS4_S5_" in defined  # bssn/include/rhs.h:39
     assert undefined == {"_ZN4bssn11BSSN_LAMBDAE", "_ZN4bssn13BSSN_LAMBDA_FE", "_ZN4bssn9ETA_CONSTE",
                          "_ZN4bssn6ETA_R0E", "_ZN4bssn15ETA_DAMPING_EXPE", "_ZN4bssn13KO_DISS_SIGMAE"}
     from oracle import pyoracle as po
@@ -99,4 +105,6 @@ def test_shim_exports_the_reference_symbol():
         ref = subprocess.run(["nm", "-D", po.REF_PARITY], capture_output=True, text=True,
                              check=True).stdout
         assert "_Z7bssnrhsPPdPPKdRKjS2_S2_PS4_S5_" in ref
+        assert "_Z20physical_constraintsPPdPPKdRKjS2_S2_PS4_S5_" in ref
+        assert "_Z11bssnrhs_sepPPdPPKdRKjS2_S2_PS4_S5_" in ref
         assert undefined <= set(re.findall(r" [DB] (_ZN4bssn\S+)", ref))

@@ -74,6 +74,19 @@ def test_oracle_vs_reference_direct(oracle_lib, n, bflag):
     assert np.all(a[:, mask] == 0) and np.all(b[:, mask] == 0)
 
 
+@pytest.mark.skipif(not po.have_reference("parity"), reason="reference build not present")
+@pytest.mark.parametrize("n,bflag", [(13, 0), (17, 0x3F), (21, 0x15)])
+def test_reference_staged_variant_equals_oracle(oracle_lib, n, bflag):
+    """bssnrhs_sep (bssn/src/rhs.cpp:392-825, the BSSN_RHS_STAGED_COMP build) computes the
+    same right-hand side as bssnrhs, so one path serves both entry points."""
+    u, blk = po.fake_block(n, (-0.45, 0.2, -0.3), 0.9 / n, bflag)
+    prm = po.params(ko_sigma=0.3)
+    a = po.interior(po.oracle_rhs(u, blk, prm), blk)
+    b = po.interior(po.ref_rhs_sep(u, blk, prm), blk)
+    mx, _ = po.rel_errors(a, b)
+    assert mx.max() < TOL
+
+
 def test_ghost_insensitive_with_all_faces(oracle_lib):
     """With every face flagged, one-sided closures never read the ghost layer."""
     u, blk = po.fake_block(15, (-0.4, 0.25, -0.15), 0.06, 0x3F)
@@ -173,3 +186,28 @@ def test_constraints_vanish_for_exact_solution(oracle_lib):
         assert np.all(c[1:] == 0.0)  # momentum: every term carries A, K or grad K
         res.append(np.abs(c[0, far]).max())
     assert res[1] < res[0] / 8.0, res
+
+
+# ---- RK4 time stepping -------------------------------------------------------------
+
+def test_oracle_rk4_is_fourth_order():
+    """Step doubling: one step of dt against two of dt/2 differ by the local error,
+    O(dt^5), so halving dt shrinks the difference ~32x."""
+    u0, blk = po.fake_block(15, (-0.4, 0.25, -0.15), 0.06, 0x3F)
+    prm = po.params(ko_sigma=0.1)
+    mask = po.interior_elements([blk], u0.shape[1])
+
+    def run(dt, n):
+        u = u0.copy()
+        rk = po.OracleRK4([blk], u.shape[1], prm)
+        rk.init(u)
+        for _ in range(n):
+            rk.step(u, dt)
+        assert np.array_equal(u[:, ~mask], u0[:, ~mask])  # ghosts never written
+        return u[:, mask]
+
+    d = []
+    for dt in (1e-3, 5e-4):
+        a, b = run(dt, 1), run(dt / 2, 2)
+        d.append((np.abs(a - b).max(axis=1) / np.abs(a).max(axis=1)).max())
+    assert 20.0 < d[0] / d[1] < 40.0, d

@@ -100,10 +100,18 @@ int enqueue_chunk(b200bssn_plan* P, DerivArgs da, AlgebraArgs aa, size_t ci, int
       bssn_constraints_kernel<float, float><<<c.range_count, kAlgebraThreads, 0, s2>>>(cc);
     else
       bssn_constraints_kernel<double, double><<<c.range_count, kAlgebraThreads, 0, s2>>>(cc);
-  } else if (mixed) {
-    bssn_algebra_kernel<float, float><<<c.range_count, kAlgebraThreads, 0, s2>>>(aa);
   } else {
-    bssn_algebra_kernel<double, double><<<c.range_count, kAlgebraThreads, 0, s2>>>(aa);
+    const unsigned g = (unsigned)c.range_count;
+#define B200_ALG(MODE)                                                                \
+  (mixed ? bssn_algebra_kernel<float, float, MODE><<<g, kAlgebraThreads, 0, s2>>>(aa) \
+         : bssn_algebra_kernel<double, double, MODE><<<g, kAlgebraThreads, 0, s2>>>(aa))
+    switch (aa.rk.mode) {
+      case RK_FIRST: B200_ALG(RK_FIRST); break;
+      case RK_MIDDLE: B200_ALG(RK_MIDDLE); break;
+      case RK_LAST: B200_ALG(RK_LAST); break;
+      default: B200_ALG(RK_NONE); break;
+    }
+#undef B200_ALG
   }
   CK(ctx, cudaGetLastError());
   if (ev) CK(ctx, cudaEventRecord(ev[4 * ci + 3], s2));
@@ -337,7 +345,7 @@ int b200bssn_plan_create_ex(b200bssn_ctx* ctx, const b200bssn_block* blocks, uin
       cur.tile_count = (int32_t)P->tiles.size() - cur.tile_begin;
       cur.range_count = (int32_t)P->ranges.size() - cur.range_begin;
       P->chunks.push_back(cur);
-      P->cap = std::max<int64_t>(P->cap, cur.points);
+      P->cap = std::max<int64_t>(P->cap, (cur.points + 31) & ~int64_t(31));
     }
     cur = ChunkRec{(int32_t)P->tiles.size(), 0, (int32_t)P->ranges.size(), 0, 0};
   };
@@ -350,7 +358,8 @@ int b200bssn_plan_create_ex(b200bssn_ctx* ctx, const b200bssn_block* blocks, uin
     const int64_t block_pts = (int64_t)I0 * I1 * (B.sz[2] - 6);
     const bool first_unit = ui == 0 || P->units[ui - 1].block != u.block;
     if (first_unit && block_pts <= capacity && cur.points + block_pts > capacity) flush();
-    if (cur.points + np > capacity) flush();
+    if (((cur.points + 31) & ~int64_t(31)) + np > capacity) flush();
+    cur.points = (cur.points + 31) & ~int64_t(31);  // slot runs start 128-byte aligned
     u.sbase = cur.points;
     cur.points += np;
     for (int j0 = 0; j0 < I1; j0 += kTileY)
@@ -426,8 +435,8 @@ int b200bssn_plan_create_ex(b200bssn_ctx* ctx, const b200bssn_block* blocks, uin
   const size_t st = precision == B200BSSN_MIXED ? sizeof(float) : sizeof(double);
   const int nbuf = P->chunks.size() > 1 ? 2 : 1;
   for (int b = 0; b < nbuf && e == cudaSuccess; ++b) {
-    e = cudaMalloc(&P->dscr[b], (size_t)kNumDerivs * P->cap * st);
-    if (e == cudaSuccess) e = cudaMalloc((void**)&P->koscr[b], (size_t)kNumVars * P->cap * sizeof(double));
+    e = cudaMalloc(&P->dscr[b], (size_t)kNumDerivs * P->cap * st + 64);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&P->koscr[b], (size_t)kNumVars * P->cap * sizeof(double) + 64);
   }
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&P->ev_fork, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaMalloc((void**)&P->d_counters, P->chunks.size() * sizeof(int));

@@ -51,7 +51,8 @@ constexpr size_t kOffTiles = kOffUnits + al256(sizeof(UnitDev) * kNoallocMaxUnit
 constexpr size_t kOffRanges = kOffTiles + al256(sizeof(TileDev) * kNoallocMaxTiles);
 constexpr size_t kOffDeriv = kOffRanges + al256(sizeof(RangeDev) * kNoallocMaxRanges);
 constexpr size_t kOffKo = kOffDeriv + al256(sizeof(double) * kNumDerivs * kNoallocMaxPoints);
-constexpr size_t kNoallocBytes = kOffKo + al256(sizeof(double) * kNumVars * kNoallocMaxPoints);
+// + 256: the algebra kernel's L2 prefetch of a slot run rounds its size up to 16 bytes
+constexpr size_t kNoallocBytes = kOffKo + al256(sizeof(double) * kNumVars * kNoallocMaxPoints) + 256;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocBytes];
 

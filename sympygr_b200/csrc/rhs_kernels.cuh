@@ -52,13 +52,16 @@ struct DerivArgs {
 // Derivative kernel: a 2.5-D streaming stencil.
 //
 // A work item is one 16x16 column tile of a unit (a z-slab of up to 48 interior
-// planes of one block) and one variable; the CTA marches along z.  Each z step brings one plane of the tile plus its 4-point x-y halo into
-// shared memory (cp.async, double-buffered: plane z+1 streams in while plane z is
+// planes of one block) and one variable; the CTA marches along z.  Each z step
+// brings one plane of the tile plus its 4-point x-y halo into shared memory
+// (cp.async into four plane buffers: three planes stream in while one is
 // differentiated).  In-plane derivatives (D_x, D_y, D_xx, D_yy, D_y(D_x), ko_x,
 // ko_y) come from that plane; the z derivatives of the variable and of its D_x
 // and D_y (D_z, D_zz, ko_z, D_z(D_x), D_z(D_y)) come from 9-deep register queues
 // that each thread keeps for its own column, so every plane is loaded once per
-// variable and no z halo is recomputed.
+// variable and no z halo is recomputed.  The item's code is instantiated twice,
+// for variables with and without second derivatives (DD), so the 13 variables
+// that need only first derivatives and KO carry no D_x/D_y queues or halo rows.
 // ---------------------------------------------------------------------------
 constexpr int kPlaneW = kTileX + 2 * kHalo;  // 24: plane width incl. halo
 constexpr int kPlaneH = kTileY + 2 * kHalo;  // 24
@@ -299,10 +302,10 @@ template <>
 struct RowsFor<float> { using type = SplitRows; };
 
 // One (column tile, variable) work item.
-template <typename ST>
+template <typename ST, bool DD>
 __device__ __forceinline__ void derive_tile(const DerivArgs& a, const TileDev t, const int v,
                                             double (*s_plane)[kPlane], void* s_dxp_raw,
-                                            LineScales* s_sc) {
+                                            double* s_kq, LineScales* s_sc) {
   using Rows = typename RowsFor<ST>::type;
   double* s_dxp = static_cast<double*>(s_dxp_raw);
   const UnitDev un = a.units[t.unit];
@@ -354,14 +357,12 @@ __device__ __forceinline__ void derive_tile(const DerivArgs& a, const TileDev t,
   }
   const int64_t plane_elems = (int64_t)nx * ny;
 
-  const int q = dd_index(v);
+  const int q = DD ? dd_index(v) : -1;
   const double* __restrict__ f = a.u[v] + B.offset;
-  double qu[kQ], qx[kQ], qy[kQ];
-  double qk[kHalo + 1];
+  double qu[kQ], qx[kQ], qy[kQ];  // planes zi-8 .. zi of u, D_x u, D_y u (D_x/D_y: DD only)
+  int kslot = 0;  // ring slot of plane zi's (ko_x + ko_y) in s_kq (five planes deep)
 #pragma unroll
   for (int k = 0; k < kQ; ++k) qu[k] = qx[k] = qy[k] = 0.0;
-#pragma unroll
-  for (int k = 0; k <= kHalo; ++k) qk[k] = 0.0;
 
   // stage plane zi into buffer b (one commit group; empty past the last needed plane)
   auto stage = [&](int zi, int b) {
@@ -374,23 +375,15 @@ __device__ __forceinline__ void derive_tile(const DerivArgs& a, const TileDev t,
     cp_async_commit();
   };
 
-  // Three plane buffers: plane zi+2 streams into the buffer plane zi-1 used,
-  // which every thread has finished with once it passes the barrier of step zi.
-  stage(zs, 0);
-  stage(zs + 1, 1);
-  for (int zi = zs, b = 0; zi < zend; ++zi, b = (b == 2 ? 0 : b + 1)) {
-    cp_async_wait<1>();
-    __syncthreads();
-    stage(zi + 2, b == 0 ? 2 : b - 1);
-    const double* P = s_plane[b];
-    const bool in_block = zi < nz;
-    const bool out_plane = zi >= k0 && zi < k0 + ez;
-    const LineScales& cx = s_sc[0];
-    const LineScales& cy = s_sc[1];
-
-    // D_x of this plane on the tile's x range and the y halo rows (only the
-    // variables with mixed derivatives need the halo rows)
-    if (q >= 0 && in_block) {
+  // Four plane buffers: plane zi+3 streams into the buffer plane zi-1 used, which
+  // every thread has finished with once it passes the barrier of step zi.  For DD
+  // variables step zi also differentiates plane zi+1 along x on the y-halo rows
+  // (into the other of two D_x buffers), so one barrier per step orders both the
+  // plane copies and the D_x rows.
+  const LineScales& cx = s_sc[0];
+  const LineScales& cy = s_sc[1];
+  auto dx_rows = [&](int zp, const double* P, double* dst) {
+    if (zp < zload) {
 #pragma unroll
       for (int r = 0; r < 2; ++r) {
         if (dx_ok[r]) {
@@ -399,11 +392,28 @@ __device__ __forceinline__ void derive_tile(const DerivArgs& a, const TileDev t,
           double w[7];
 #pragma unroll
           for (int k = 0; k < 7; ++k) w[k] = p[k - 3];
-          s_dxp[yy * kTileX + dxx] = dcl ? cl_d1(p, 1, dpi, nx, lox, hix, cx) : Rows::d1_field(w, 3, cx);
+          dst[yy * kTileX + dxx] = dcl ? cl_d1(p, 1, dpi, nx, lox, hix, cx) : Rows::d1_field(w, 3, cx);
         }
       }
-      __syncthreads();
     }
+  };
+  stage(zs, 0);
+  stage(zs + 1, 1);
+  stage(zs + 2, 2);
+  if (DD) {
+    cp_async_wait<2>();
+    __syncthreads();  // plane zs (and the line scales) visible to every thread
+    dx_rows(zs, s_plane[0], s_dxp);
+  }
+  for (int zi = zs, b = 0; zi < zend; ++zi, b = (b + 1) & 3) {
+    cp_async_wait<1>();
+    __syncthreads();
+    stage(zi + 3, (b + 3) & 3);
+    const double* P = s_plane[b];
+    const double* Dxp = s_dxp + ((zi - zs) & 1) * (kDxRows * kTileX);
+    const bool in_block = zi < nz;
+    const bool out_plane = zi >= k0 && zi < k0 + ez;
+    if (DD) dx_rows(zi + 1, s_plane[(b + 1) & 3], s_dxp + ((zi + 1 - zs) & 1) * (kDxRows * kTileX));
 
     double dx = 0.0, dy = 0.0, kxy = 0.0, u0 = 0.0;
     if (active && in_block) {
@@ -415,21 +425,21 @@ __device__ __forceinline__ void derive_tile(const DerivArgs& a, const TileDev t,
         wx[k] = pc[k - 3];
         wy[k] = pc[(k - 3) * kPlaneW];
       }
-      dx = q >= 0 ? s_dxp[(ty + kHalo) * kTileX + tx]
+      dx = DD ? Dxp[(ty + kHalo) * kTileX + tx]
                   : (clx ? cl_d1(pc, 1, gi, nx, lox, hix, cx) : Rows::d1_field(wx, 3, cx));
       dy = cly ? cl_d1(pc, kPlaneW, gj, ny, loy, hiy, cy) : Rows::d1_field(wy, 3, cy);
       if (out_plane) {
         const int lp = lp_col + plane_pts * (zi - k0);
         const double kx = clx ? cl_ko(pc, 1, gi, nx, lox, hix, cx) : Rows::ko(wx, 3, cx);
         const double ky = cly ? cl_ko(pc, kPlaneW, gj, ny, loy, hiy, cy) : Rows::ko(wy, 3, cy);
-        kxy = __dadd_rn(kx, ky);
+        s_kq[kslot * kDerivThreads + threadIdx.x] = __dadd_rn(kx, ky);
         put_slot<ST>(a, 3 * v + 0, lp, dx);
         put_slot<ST>(a, 3 * v + 1, lp, dy);
-        if (q >= 0) {
+        if (DD) {
           const int s0 = 72 + 6 * q;
           put_slot<ST>(a, s0 + 0, lp, clx ? cl_d2(pc, 1, gi, nx, lox, hix, cx) : (double)Rows::d2(wx, 3, cx));
           put_slot<ST>(a, s0 + 3, lp, cly ? cl_d2(pc, kPlaneW, gj, ny, loy, hiy, cy) : (double)Rows::d2(wy, 3, cy));
-          const double* pd = s_dxp + (ty + kHalo) * kTileX + tx;
+          const double* pd = Dxp + (ty + kHalo) * kTileX + tx;
           double wd[7];
 #pragma unroll
           for (int k = 0; k < 7; ++k) wd[k] = pd[(k - 3) * kTileX];
@@ -439,9 +449,14 @@ __device__ __forceinline__ void derive_tile(const DerivArgs& a, const TileDev t,
       }
     }
     q_push(qu, u0);
-    q_push(qx, dx);
-    q_push(qy, dy);
-    q_push(qk, kxy);
+    if (DD) {
+      q_push(qx, dx);
+      q_push(qy, dy);
+    }
+    // (ko_x + ko_y) of plane zi - 4, written four steps ago into slot kslot - 4 (mod 5)
+    const int kold = kslot == kHalo ? 0 : kslot + 1;
+    kxy = s_kq[kold * kDerivThreads + threadIdx.x];
+    kslot = kold;
 
     // z derivatives of plane zo = zi - 4, whose +-4 neighbourhood is now queued
     const int zo = zi - kHalo;
@@ -452,8 +467,8 @@ __device__ __forceinline__ void derive_tile(const DerivArgs& a, const TileDev t,
       const bool zcl = zc >= 0;
       put_slot<ST>(a, 3 * v + 2, lp, zcl ? zq_d1_closure(qu, zc, cz) : (double)Rows::d1(qu, 4, cz));
       // rhs.cpp:332-369 sums (ko_x + ko_y) + ko_z
-      a.koscr[v * a.cap + lp] = __dadd_rn(qk[0], zcl ? zq_ko_closure(qu, zc, cz) : Rows::ko(qu, 4, cz));
-      if (q >= 0) {
+      a.koscr[v * a.cap + lp] = __dadd_rn(kxy, zcl ? zq_ko_closure(qu, zc, cz) : Rows::ko(qu, 4, cz));
+      if (DD) {
         const int s0 = 72 + 6 * q;
         put_slot<ST>(a, s0 + 5, lp, zcl ? (double)zq_d2_closure(qu, zc, cz) : (double)Rows::d2(qu, 4, cz));
         put_slot<ST>(a, s0 + 2, lp, zcl ? (double)zq_d1_closure(qx, zc, cz) : (double)Rows::d1(qx, 4, cz));
@@ -472,8 +487,9 @@ __device__ __forceinline__ void derive_tile(const DerivArgs& a, const TileDev t,
 template <typename ST>
 __global__ void __launch_bounds__(kDerivThreads, 2)
 bssn_derivs_kernel(const __grid_constant__ DerivArgs a) {
-  __shared__ double s_plane[3][kPlane];            // staged planes (tile + x-y halo)
-  __shared__ double s_dxp[kDxRows * kTileX];       // D_x of the current plane, y halo rows (FP64)
+  __shared__ double s_plane[4][kPlane];
+  __shared__ double s_dxp[2 * kDxRows * kTileX];
+  __shared__ double s_kq[(kHalo + 1) * kDerivThreads];
   __shared__ LineScales s_sc[3];
   __shared__ int s_item;
   for (;;) {
@@ -483,8 +499,12 @@ bssn_derivs_kernel(const __grid_constant__ DerivArgs a) {
     const int item = s_item;
     if (item >= a.tile_count * kNumVars) break;
     // items run tile-major: the longest tiles (listed first) are all taken first
-    derive_tile<ST>(a, a.tiles[a.tile_base + item / kNumVars], item % kNumVars, s_plane, s_dxp,
-                    s_sc);
+    const TileDev t = a.tiles[a.tile_base + item / kNumVars];
+    const int v = item % kNumVars;
+    if (dd_index(v) >= 0)
+      derive_tile<ST, true>(a, t, v, s_plane, s_dxp, s_kq, s_sc);
+    else
+      derive_tile<ST, false>(a, t, v, s_plane, s_dxp, s_kq, s_sc);
   }
 }
 
@@ -525,21 +545,28 @@ struct PointIn {
   }
 };
 
-// Stores the right-hand side k of variable v at element pp: to the RHS arrays, or
-// through the RK4 stage update.
-// Any mode other than the three stage modes stores the RHS.
+// Stores the right-hand side k of variable v at element pp: to the RHS arrays
+// (MODE RK_NONE) or through one RK4 stage update.  The mode is a template
+// parameter so each instantiation is straight-line code: a run-time branch per
+// output splits the generated algebra into basic blocks the scheduler cannot
+// interleave across (measured: the algebra kernel ran 2x slower).
+template <int MODE>
 __device__ __forceinline__ void store_rhs(const AlgebraArgs& a, int v, int64_t pp, double k) {
   const RkStage& rk = a.rk;
-  if (rk.mode == RK_LAST) {
+  if constexpr (MODE == RK_LAST) {
     rk.base[v][pp] = rk.base[v][pp] + rk.acc[v][pp] + rk.w * k;
-  } else if (rk.mode == RK_FIRST || rk.mode == RK_MIDDLE) {
-    rk.acc[v][pp] = rk.mode == RK_FIRST ? rk.w * k : rk.acc[v][pp] + rk.w * k;
+  } else if constexpr (MODE == RK_FIRST) {
+    rk.acc[v][pp] = rk.w * k;
+    rk.next[v][pp] = __ldg(rk.base[v] + pp) + rk.c * k;
+  } else if constexpr (MODE == RK_MIDDLE) {
+    rk.acc[v][pp] = rk.acc[v][pp] + rk.w * k;
     rk.next[v][pp] = __ldg(rk.base[v] + pp) + rk.c * k;
   } else {
     a.rhs[v][pp] = k;
   }
 }
 
+template <int MODE>
 struct PointSink {
   const AlgebraArgs* a;
   int64_t pp;
@@ -547,14 +574,32 @@ struct PointSink {
   template <typename RT>
   __device__ __forceinline__ void put(int v, RT val) {
     // rhs += sigma * (ko_x + ko_y + ko_z), rounded as rhs.cpp:332-369 rounds it
-    store_rhs(*a, v, pp, __dadd_rn((double)val, __dmul_rn(a->ko_sigma, __ldg(a->koscr + v * a->cap + lp))));
+    store_rhs<MODE>(*a, v, pp, __dadd_rn((double)val, __dmul_rn(a->ko_sigma, __ldg(a->koscr + v * a->cap + lp))));
   }
 };
 
-template <typename RT, typename ST>
+__device__ __forceinline__ void prefetch_l2_bulk(const void* p, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
+template <typename RT, typename ST, int MODE = RK_NONE>
 __global__ void __launch_bounds__(kAlgebraThreads, 2)
 bssn_algebra_kernel(const __grid_constant__ AlgebraArgs a) {
   const RangeDev rg = a.ranges[a.range_base + blockIdx.x];
+  {
+    // pull this CTA's run of every scratch slot into L2 with one bulk prefetch per
+    // slot, so the per-point loads below hit L2 instead of waiting on DRAM
+    const UnitDev un0 = a.units[rg.unit];
+    const int lp0 = (int)un0.sbase + rg.start;
+    const uint32_t bd = ((uint32_t)rg.count * (uint32_t)sizeof(ST) + 15u) & ~15u;
+    const uint32_t bk = ((uint32_t)rg.count * 8u + 15u) & ~15u;
+    for (int s = threadIdx.x; s < kNumDerivs + kNumVars; s += kAlgebraThreads) {
+      const char* p = s < kNumDerivs
+                          ? reinterpret_cast<const char*>(static_cast<const ST*>(a.dscr) + (size_t)s * a.cap + lp0)
+                          : reinterpret_cast<const char*>(a.koscr + (size_t)(s - kNumDerivs) * a.cap + lp0);
+      if ((reinterpret_cast<uintptr_t>(p) & 15u) == 0) prefetch_l2_bulk(p, s < kNumDerivs ? bd : bk);
+    }
+  }
   if ((int)threadIdx.x >= rg.count) return;
   const UnitDev un = a.units[rg.unit];
   const BlockDev& B = a.blocks[un.block];
@@ -590,7 +635,7 @@ bssn_algebra_kernel(const __grid_constant__ AlgebraArgs a) {
       t = __dadd_rn(t, __dmul_rn(z, dzf));
       t = __dadd_rn(t, __dmul_rn(bc_falloff(v), __dsub_rn(f, bc_asymptotic(v))));
       const double val = __dmul_rn(-inv_r, t);
-      store_rhs(a, v, pp, __dadd_rn(val, __dmul_rn(a.ko_sigma, __ldg(a.koscr + v * a.cap + lp))));
+      store_rhs<MODE>(a, v, pp, __dadd_rn(val, __dmul_rn(a.ko_sigma, __ldg(a.koscr + v * a.cap + lp))));
     }
     return;
   }
@@ -600,7 +645,7 @@ bssn_algebra_kernel(const __grid_constant__ AlgebraArgs a) {
   if (r_coord >= a.eta_r0) eta *= pow(a.eta_r0 / r_coord, a.eta_damping_exp);
 
   PointIn<RT, ST> in{&a, pp, lp};
-  PointSink sink{&a, pp, lp};
+  PointSink<MODE> sink{&a, pp, lp};
   if constexpr (sizeof(RT) == 8) {
     bssn_rhs_algebra<RT>(in, sink, a.prm64, (RT)eta);
   } else {

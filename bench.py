@@ -47,7 +47,7 @@ MIXED_BAR = 1e-6
 SCRATCH_BYTES = {"fp64": 138 * 8 + 24 * 8, "mixed": 138 * 4 + 24 * 8}
 # DRAM bytes per interior point of each kernel measured by ncu on a large-block case
 # (profiles/ncu_derivs_algebra_large_blocks.md): derivative / algebra kernel.
-NCU_TRAFFIC_PER_POINT = {"mixed": (1259.2, 1124.6), "fp64": (1850.3, 1792.4)}
+NCU_TRAFFIC_PER_POINT = {"mixed": (1242.2, 1133.9), "fp64": (1802.4, 2053.4)}
 
 
 def _env_int(k, d):

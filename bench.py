@@ -50,6 +50,28 @@ SCRATCH_BYTES = {"fp64": 138 * 8 + 24 * 8, "mixed": 138 * 4 + 24 * 8}
 NCU_TRAFFIC_PER_POINT = {"mixed": (1242.2, 1133.9), "fp64": (1802.4, 2053.4)}
 
 
+def max_over_ranks(value: float, dist=None, device="cuda") -> float:
+    """The largest `value` over all ranks (every rank receives it); `dist` None: one process."""
+    if dist is None:
+        return value
+    import torch
+
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.item()
+
+
+def sum_over_ranks(value: int, dist=None, device="cuda") -> int:
+    """The sum of an integer count over all ranks; `dist` None: one process."""
+    if dist is None:
+        return value
+    import torch
+
+    t = torch.tensor([int(value)], dtype=torch.int64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return int(t.item())
+
+
 def _env_int(k, d):
     try:
         return int(os.environ.get(k, d))
@@ -275,12 +297,7 @@ def main():
         e1.synchronize()
         torch.cuda.synchronize()
         barrier()
-        ms = e0.elapsed_time(e1)
-        if dist is not None:
-            t = torch.tensor([ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = t.item()
-        return ms / k
+        return max_over_ranks(e0.elapsed_time(e1), dist) / k
 
     for prec in (sg.MIXED, sg.FP64):
         for _ in range(args.warmup):
@@ -319,7 +336,7 @@ def main():
     peak32 = capi.fma_peak_tflops(local_rank, sg.MIXED)
 
     launches = plans[sg.MIXED].launches * args.steps
-    total_pts = npts * world
+    total_pts = sum_over_ranks(npts, dist)  # each rank evaluates its own batch
     val_mixed = total_pts / (ms_mixed * 1e-3) / 1e6
     val_fp64 = total_pts / (ms_fp64 * 1e-3) / 1e6
 
@@ -367,11 +384,7 @@ def main():
             plans[sg.MIXED].rhs_host(RH, UH, span, p_host)
         e1.record(stream)
         e1.synchronize()
-        ms = e0.elapsed_time(e1) / args.e2e_steps
-        if dist is not None:
-            t = torch.tensor([ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = t.item()
+        ms = max_over_ranks(e0.elapsed_time(e1) / args.e2e_steps, dist)
         nbytes = 24 * span * 8
         del u_h, r_h
         e2e = {"value": round(total_pts / (ms * 1e-3) / 1e6, 3), "unit": UNIT,

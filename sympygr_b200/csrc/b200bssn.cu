@@ -102,8 +102,12 @@ int enqueue_chunk(b200bssn_plan* P, DerivArgs da, AlgebraArgs aa, size_t ci, int
       bssn_constraints_kernel<double, double><<<c.range_count, kAlgebraThreads, 0, s2>>>(cc);
   } else {
     const unsigned g = (unsigned)c.range_count;
-#define B200_ALG(MODE)                                                                \
-  (mixed ? bssn_algebra_kernel<float, float, MODE><<<g, kAlgebraThreads, 0, s2>>>(aa) \
+    const int ntasks = c.range_count * (kAlgebraThreads / kStageW);
+    const unsigned gs = (unsigned)std::max(1, std::min(P->alg_grid, (ntasks + 3) / 4));
+    // MIXED: the staged persistent kernel; FP64 (whose slots would need twice the
+    // shared memory): one CTA per range
+#define B200_ALG(MODE)                                                                              \
+  (mixed ? bssn_algebra_staged_kernel<MODE><<<gs, kAlgebraThreads, kStageSmemBytes, s2>>>(aa, ntasks) \
          : bssn_algebra_kernel<double, double, MODE><<<g, kAlgebraThreads, 0, s2>>>(aa))
     switch (aa.rk.mode) {
       case RK_FIRST: B200_ALG(RK_FIRST); break;
@@ -164,6 +168,14 @@ int b200bssn::host::launch_plan(b200bssn_plan* P, double* const* rhs, const doub
 namespace {
 
 int set_kernel_attributes(b200bssn_ctx* ctx) {
+  CK(ctx, cudaFuncSetAttribute(bssn_algebra_staged_kernel<RK_NONE>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStageSmemBytes));
+  CK(ctx, cudaFuncSetAttribute(bssn_algebra_staged_kernel<RK_FIRST>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStageSmemBytes));
+  CK(ctx, cudaFuncSetAttribute(bssn_algebra_staged_kernel<RK_MIDDLE>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStageSmemBytes));
+  CK(ctx, cudaFuncSetAttribute(bssn_algebra_staged_kernel<RK_LAST>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStageSmemBytes));
   CK(ctx, cudaFuncSetAttribute(bssn_derivs_kernel<double>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDerivSmemBytes));
   CK(ctx, cudaFuncSetAttribute(bssn_derivs_kernel<float>,
@@ -425,6 +437,10 @@ int b200bssn_plan_create_ex(b200bssn_ctx* ctx, const b200bssn_block* blocks, uin
         kDerivThreads, kDerivSmemBytes);
     if (o.deriv_ctas_per_sm) per_sm = std::min<int>(per_sm, (int)o.deriv_ctas_per_sm);
     P->deriv_grid = std::max(1, sms * std::max(1, per_sm));
+    int alg_per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&alg_per_sm, bssn_algebra_staged_kernel<RK_NONE>,
+                                                  kAlgebraThreads, kStageSmemBytes);
+    P->alg_grid = std::max(1, sms * std::max(1, alg_per_sm));
   }
 
   const size_t nb = P->blocks.size() * sizeof(BlockDev), nu = P->units.size() * sizeof(UnitDev),
@@ -435,8 +451,10 @@ int b200bssn_plan_create_ex(b200bssn_ctx* ctx, const b200bssn_block* blocks, uin
   const size_t st = precision == B200BSSN_MIXED ? sizeof(float) : sizeof(double);
   const int nbuf = P->chunks.size() > 1 ? 2 : 1;
   for (int b = 0; b < nbuf && e == cudaSuccess; ++b) {
-    e = cudaMalloc(&P->dscr[b], (size_t)kNumDerivs * P->cap * st + 64);
-    if (e == cudaSuccess) e = cudaMalloc((void**)&P->koscr[b], (size_t)kNumVars * P->cap * sizeof(double) + 64);
+    // + 512 B: the algebra kernels' copies and prefetches of a slot run are whole
+    // 16-byte chunks or 32-point columns and may read past the last run's end
+    e = cudaMalloc(&P->dscr[b], (size_t)kNumDerivs * P->cap * st + 512);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&P->koscr[b], (size_t)kNumVars * P->cap * sizeof(double) + 512);
   }
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&P->ev_fork, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaMalloc((void**)&P->d_counters, P->chunks.size() * sizeof(int));

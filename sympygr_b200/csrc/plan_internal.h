@@ -72,6 +72,7 @@ struct b200bssn_plan {
   std::vector<uint64_t> part;
   std::vector<cudaEvent_t> ev_in;  // per chunk: upload done
   int deriv_grid = 0;         // resident CTAs of the persistent derivative kernel
+  int alg_grid = 0;           // resident CTAs of the persistent staged algebra kernel (MIXED)
   // host-batch staging (allocated on first host call)
   double* st_u = nullptr;
   double* st_rhs = nullptr;

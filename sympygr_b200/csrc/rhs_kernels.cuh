@@ -510,6 +510,11 @@ bssn_derivs_kernel(const __grid_constant__ DerivArgs a) {
 
 constexpr size_t kDerivSmemBytes = 0;  // all shared memory is static
 
+constexpr int kStageW = 32;  // points per task of the staged algebra kernel (one warp)
+constexpr size_t kStageBytesPerWarp = (size_t)kNumDerivs * kStageW * sizeof(float) +
+                                      (size_t)kNumVars * kStageW * sizeof(double);
+constexpr size_t kStageSmemBytes = (kAlgebraThreads / 32) * kStageBytesPerWarp;  // 95,232 B
+
 struct AlgebraArgs {
   const double* u[kNumVars];
   double* rhs[kNumVars];
@@ -534,15 +539,33 @@ __device__ __forceinline__ double bc_asymptotic(int v) {
   return (v == 0 || v == 1 || v == 12 || v == 15 || v == 17) ? 1.0 : 0.0;
 }
 
-template <typename RT, typename ST>
+// Where an algebra thread reads its point's derivative slots and KO sums: straight
+// from the scratch arrays in global memory, or from a copy its warp staged in
+// shared memory (one 32-point column per slot).
+template <typename ST>
+struct GlobalScratch {
+  const ST* d;       // dscr + lp
+  const double* ko;  // koscr + lp
+  int cap;
+  __device__ __forceinline__ ST dv(int s) const { return __ldg(d + s * cap); }
+  __device__ __forceinline__ double kov(int v) const { return __ldg(ko + v * cap); }
+};
+
+template <typename ST>
+struct SharedScratch {
+  const ST* d;       // this lane's column: d[s * kStageW]
+  const double* ko;  // ko[v * kStageW]
+  __device__ __forceinline__ ST dv(int s) const { return d[s * kStageW]; }
+  __device__ __forceinline__ double kov(int v) const { return ko[v * kStageW]; }
+};
+
+template <typename RT, class Src>
 struct PointIn {
   const AlgebraArgs* a;
   int64_t pp;   // element index of the point in the variable arrays
-  int lp;       // scratch index
+  Src src;
   __device__ __forceinline__ RT u(int v) const { return (RT)__ldg(a->u[v] + pp); }
-  __device__ __forceinline__ RT d(int s) const {
-    return (RT)__ldg(static_cast<const ST*>(a->dscr) + s * a->cap + lp);
-  }
+  __device__ __forceinline__ RT d(int s) const { return (RT)src.dv(s); }
 };
 
 // Stores the right-hand side k of variable v at element pp: to the RHS arrays
@@ -566,15 +589,15 @@ __device__ __forceinline__ void store_rhs(const AlgebraArgs& a, int v, int64_t p
   }
 }
 
-template <int MODE>
+template <int MODE, class Src>
 struct PointSink {
   const AlgebraArgs* a;
   int64_t pp;
-  int lp;
+  Src src;
   template <typename RT>
   __device__ __forceinline__ void put(int v, RT val) {
     // rhs += sigma * (ko_x + ko_y + ko_z), rounded as rhs.cpp:332-369 rounds it
-    store_rhs<MODE>(*a, v, pp, __dadd_rn((double)val, __dmul_rn(a->ko_sigma, __ldg(a->koscr + v * a->cap + lp))));
+    store_rhs<MODE>(*a, v, pp, __dadd_rn((double)val, __dmul_rn(a->ko_sigma, src.kov(v))));
   }
 };
 
@@ -582,34 +605,17 @@ __device__ __forceinline__ void prefetch_l2_bulk(const void* p, uint32_t bytes) 
   asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
 }
 
-template <typename RT, typename ST, int MODE = RK_NONE>
-__global__ void __launch_bounds__(kAlgebraThreads, 2)
-bssn_algebra_kernel(const __grid_constant__ AlgebraArgs a) {
-  const RangeDev rg = a.ranges[a.range_base + blockIdx.x];
-  {
-    // pull this CTA's run of every scratch slot into L2 with one bulk prefetch per
-    // slot, so the per-point loads below hit L2 instead of waiting on DRAM
-    const UnitDev un0 = a.units[rg.unit];
-    const int lp0 = (int)un0.sbase + rg.start;
-    const uint32_t bd = ((uint32_t)rg.count * (uint32_t)sizeof(ST) + 15u) & ~15u;
-    const uint32_t bk = ((uint32_t)rg.count * 8u + 15u) & ~15u;
-    for (int s = threadIdx.x; s < kNumDerivs + kNumVars; s += kAlgebraThreads) {
-      const char* p = s < kNumDerivs
-                          ? reinterpret_cast<const char*>(static_cast<const ST*>(a.dscr) + (size_t)s * a.cap + lp0)
-                          : reinterpret_cast<const char*>(a.koscr + (size_t)(s - kNumDerivs) * a.cap + lp0);
-      if ((reinterpret_cast<uintptr_t>(p) & 15u) == 0) prefetch_l2_bulk(p, s < kNumDerivs ? bd : bk);
-    }
-  }
-  if ((int)threadIdx.x >= rg.count) return;
-  const UnitDev un = a.units[rg.unit];
+// The right-hand side of one interior point: local index lpu of unit `un`, inputs
+// through `src`.
+template <typename RT, int MODE, class Src>
+__device__ __forceinline__ void algebra_point(const AlgebraArgs& a, const UnitDev& un, int lpu,
+                                              const Src& src) {
   const BlockDev& B = a.blocks[un.block];
   const int nx = B.sz[0], ny = B.sz[1];
   const int I0 = nx - 6, I1 = ny - 6;
-  const int lpu = rg.start + threadIdx.x;
   const int lx = lpu % I0, rr = lpu / I0, ly = rr % I1, lz = rr / I1;
   const int i = lx + 3, j = ly + 3, k = lz + 3 + un.k0;
   const int64_t pp = B.offset + i + (int64_t)nx * (j + (int64_t)ny * k);
-  const int lp = (int)un.sbase + lpu;
   // coordinates as bssnrhs forms them (pmin + i*h, two roundings, rhs.cpp:207-213)
   const double x = __dadd_rn(B.pmin[0], __dmul_rn((double)i, B.h[0]));
   const double y = __dadd_rn(B.pmin[1], __dmul_rn((double)j, B.h[1]));
@@ -623,19 +629,18 @@ bssn_algebra_kernel(const __grid_constant__ AlgebraArgs a) {
     // bssn_bcs (rhs.cpp:833-977) replaces the algebra on face planes; KO is added
     // afterwards (rhs.cpp:323-369).
     const double inv_r = 1.0 / sqrt(r2);
-    const ST* ds = static_cast<const ST*>(a.dscr);
 #pragma unroll 1
     for (int v = 0; v < kNumVars; ++v) {
       const double f = __ldg(a.u[v] + pp);
-      const double dxf = (double)__ldg(ds + (3 * v + 0) * a.cap + lp);
-      const double dyf = (double)__ldg(ds + (3 * v + 1) * a.cap + lp);
-      const double dzf = (double)__ldg(ds + (3 * v + 2) * a.cap + lp);
+      const double dxf = (double)src.dv(3 * v + 0);
+      const double dyf = (double)src.dv(3 * v + 1);
+      const double dzf = (double)src.dv(3 * v + 2);
       double t = __dmul_rn(x, dxf);
       t = __dadd_rn(t, __dmul_rn(y, dyf));
       t = __dadd_rn(t, __dmul_rn(z, dzf));
       t = __dadd_rn(t, __dmul_rn(bc_falloff(v), __dsub_rn(f, bc_asymptotic(v))));
       const double val = __dmul_rn(-inv_r, t);
-      store_rhs<MODE>(a, v, pp, __dadd_rn(val, __dmul_rn(a.ko_sigma, __ldg(a.koscr + v * a.cap + lp))));
+      store_rhs<MODE>(a, v, pp, __dadd_rn(val, __dmul_rn(a.ko_sigma, src.kov(v))));
     }
     return;
   }
@@ -644,12 +649,107 @@ bssn_algebra_kernel(const __grid_constant__ AlgebraArgs a) {
   double eta = a.eta_const;
   if (r_coord >= a.eta_r0) eta *= pow(a.eta_r0 / r_coord, a.eta_damping_exp);
 
-  PointIn<RT, ST> in{&a, pp, lp};
-  PointSink<MODE> sink{&a, pp, lp};
+  PointIn<RT, Src> in{&a, pp, src};
+  PointSink<MODE, Src> sink{&a, pp, src};
   if constexpr (sizeof(RT) == 8) {
     bssn_rhs_algebra<RT>(in, sink, a.prm64, (RT)eta);
   } else {
     bssn_rhs_algebra<RT>(in, sink, a.prm32, (RT)eta);
+  }
+}
+
+// One CTA per range of up to 128 consecutive points of a unit, one thread per point,
+// inputs loaded from global memory as the generated code needs them.
+template <typename RT, typename ST, int MODE = RK_NONE>
+__global__ void __launch_bounds__(kAlgebraThreads, 2)
+bssn_algebra_kernel(const __grid_constant__ AlgebraArgs a) {
+  const RangeDev rg = a.ranges[a.range_base + blockIdx.x];
+  const UnitDev un = a.units[rg.unit];
+  {
+    // pull this CTA's run of every scratch slot into L2 with one bulk prefetch per
+    // slot, so the per-point loads below hit L2 instead of waiting on DRAM
+    const int lp0 = (int)un.sbase + rg.start;
+    const uint32_t bd = ((uint32_t)rg.count * (uint32_t)sizeof(ST) + 15u) & ~15u;
+    const uint32_t bk = ((uint32_t)rg.count * 8u + 15u) & ~15u;
+    for (int s = threadIdx.x; s < kNumDerivs + kNumVars; s += kAlgebraThreads) {
+      const char* p = s < kNumDerivs
+                          ? reinterpret_cast<const char*>(static_cast<const ST*>(a.dscr) + (size_t)s * a.cap + lp0)
+                          : reinterpret_cast<const char*>(a.koscr + (size_t)(s - kNumDerivs) * a.cap + lp0);
+      if ((reinterpret_cast<uintptr_t>(p) & 15u) == 0) prefetch_l2_bulk(p, s < kNumDerivs ? bd : bk);
+    }
+  }
+  if ((int)threadIdx.x >= rg.count) return;
+  const int lpu = rg.start + threadIdx.x;
+  const int lp = (int)un.sbase + lpu;
+  const GlobalScratch<ST> src{static_cast<const ST*>(a.dscr) + lp, a.koscr + lp, a.cap};
+  algebra_point<RT, MODE>(a, un, lpu, src);
+}
+
+
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem_src) : "memory");
+}
+
+__device__ __forceinline__ void prefetch_l2(const void* p) {
+  asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
+// Staged algebra kernel (MIXED): persistent warps, each taking 32-point tasks
+// (quarters of a range) round-robin.  A task first copies its points' 138 FP32
+// slots and 24 KO sums into the warp's shared-memory buffer with 16-byte cp.async
+// (eight lanes per 128-byte slot column, four slots per instruction; the planner
+// starts every unit's scratch run on a 32-point boundary and pads the scratch, so
+// the copies are aligned and in bounds) and prefetches the 24 state values into L2,
+// then runs the algebra reading shared memory: the loads that kept the
+// one-CTA-per-range version waiting on L2/DRAM become shared-memory loads, and while
+// one warp waits for its copies the others compute.
+template <int MODE>
+__global__ void __launch_bounds__(kAlgebraThreads, 2)
+bssn_algebra_staged_kernel(const __grid_constant__ AlgebraArgs a, int ntasks) {
+  extern __shared__ __align__(16) unsigned char s_stage[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float* sd = reinterpret_cast<float*>(s_stage + warp * kStageBytesPerWarp);
+  double* sk = reinterpret_cast<double*>(s_stage + warp * kStageBytesPerWarp +
+                                         kNumDerivs * kStageW * sizeof(float));
+  const int nwarps = gridDim.x * (kAlgebraThreads / 32);
+  for (int t = blockIdx.x * (kAlgebraThreads / 32) + warp; t < ntasks; t += nwarps) {
+    const RangeDev rg = a.ranges[a.range_base + (t >> 2)];
+    const int start = (t & 3) * kStageW;
+    if (start >= rg.count) continue;
+    const UnitDev un = a.units[rg.unit];
+    const int lp0 = (int)un.sbase + rg.start + start;  // multiple of 32
+    const int lpu = rg.start + start + lane;
+    const bool valid = start + lane < rg.count;
+    if (valid) {
+      const BlockDev& B = a.blocks[un.block];
+      const int I0 = B.sz[0] - 6, I1 = B.sz[1] - 6;
+      const int lx = lpu % I0, rr = lpu / I0, ly = rr % I1, lz = rr / I1;
+      const int64_t pp = B.offset + (lx + 3) + (int64_t)B.sz[0] * ((ly + 3) + (int64_t)B.sz[1] * (lz + 3 + un.k0));
+#pragma unroll
+      for (int v = 0; v < kNumVars; ++v) prefetch_l2(a.u[v] + pp);
+    }
+    __syncwarp();  // every lane is done reading the previous task's buffer
+    {
+      // slots: lane = 8 * (slot % 4) + chunk; chunk c holds points 4c .. 4c+3
+      const int sub = lane >> 3, c = lane & 7;
+      const float* d = static_cast<const float*>(a.dscr) + lp0 + 4 * c;
+#pragma unroll 5
+      for (int s = sub; s < kNumDerivs; s += 4)
+        cp_async16(sd + s * kStageW + 4 * c, d + (size_t)s * a.cap);
+      // KO sums: lane = 16 * (var % 2) + chunk; chunk c holds points 2c, 2c+1
+      const int vk = lane >> 4, ck = lane & 15;
+      const double* ko = a.koscr + lp0 + 2 * ck;
+#pragma unroll 4
+      for (int v = vk; v < kNumVars; v += 2) cp_async16(sk + v * kStageW + 2 * ck, ko + (size_t)v * a.cap);
+    }
+    cp_async_commit();
+    cp_async_wait<0>();
+    __syncwarp();  // the copies of every lane are visible to the whole warp
+    if (valid) {
+      const SharedScratch<float> src{sd + lane, sk + lane};
+      algebra_point<float, MODE>(a, un, lpu, src);
+    }
   }
 }
 

@@ -101,14 +101,14 @@ int enqueue_chunk(b200bssn_plan* P, DerivArgs da, AlgebraArgs aa, size_t ci, int
     else
       bssn_constraints_kernel<double, double><<<c.range_count, kAlgebraThreads, 0, s2>>>(cc);
   } else {
-    const unsigned g = (unsigned)c.range_count;
     const int ntasks = c.range_count * (kAlgebraThreads / kStageW);
-    const unsigned gs = (unsigned)std::max(1, std::min(P->alg_grid, (ntasks + 3) / 4));
-    // MIXED: the staged persistent kernel; FP64 (whose slots would need twice the
-    // shared memory): one CTA per range
-#define B200_ALG(MODE)                                                                              \
-  (mixed ? bssn_algebra_staged_kernel<MODE><<<gs, kAlgebraThreads, kStageSmemBytes, s2>>>(aa, ntasks) \
-         : bssn_algebra_kernel<double, double, MODE><<<g, kAlgebraThreads, 0, s2>>>(aa))
+    const unsigned gs = (unsigned)std::max(1, std::min(P->alg_grid, ntasks));
+    // the staged persistent kernel: each warp takes 32-point tasks round-robin
+#define B200_ALG(MODE)                                                                          \
+  (mixed ? bssn_algebra_staged_kernel<float, MODE>                                              \
+               <<<gs, StageCfg<float>::kThreads, StageCfg<float>::kSmemBytes, s2>>>(aa, ntasks) \
+         : bssn_algebra_staged_kernel<double, MODE>                                             \
+               <<<gs, StageCfg<double>::kThreads, StageCfg<double>::kSmemBytes, s2>>>(aa, ntasks))
     switch (aa.rk.mode) {
       case RK_FIRST: B200_ALG(RK_FIRST); break;
       case RK_MIDDLE: B200_ALG(RK_MIDDLE); break;
@@ -168,14 +168,19 @@ int b200bssn::host::launch_plan(b200bssn_plan* P, double* const* rhs, const doub
 namespace {
 
 int set_kernel_attributes(b200bssn_ctx* ctx) {
-  CK(ctx, cudaFuncSetAttribute(bssn_algebra_staged_kernel<RK_NONE>,
-                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStageSmemBytes));
-  CK(ctx, cudaFuncSetAttribute(bssn_algebra_staged_kernel<RK_FIRST>,
-                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStageSmemBytes));
-  CK(ctx, cudaFuncSetAttribute(bssn_algebra_staged_kernel<RK_MIDDLE>,
-                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStageSmemBytes));
-  CK(ctx, cudaFuncSetAttribute(bssn_algebra_staged_kernel<RK_LAST>,
-                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStageSmemBytes));
+#define B200_STAGE_ATTR(ST, MODE)                                                        \
+  CK(ctx, cudaFuncSetAttribute(bssn_algebra_staged_kernel<ST, MODE>,                      \
+                               cudaFuncAttributeMaxDynamicSharedMemorySize,               \
+                               (int)StageCfg<ST>::kSmemBytes))
+  B200_STAGE_ATTR(float, RK_NONE);
+  B200_STAGE_ATTR(float, RK_FIRST);
+  B200_STAGE_ATTR(float, RK_MIDDLE);
+  B200_STAGE_ATTR(float, RK_LAST);
+  B200_STAGE_ATTR(double, RK_NONE);
+  B200_STAGE_ATTR(double, RK_FIRST);
+  B200_STAGE_ATTR(double, RK_MIDDLE);
+  B200_STAGE_ATTR(double, RK_LAST);
+#undef B200_STAGE_ATTR
   CK(ctx, cudaFuncSetAttribute(bssn_derivs_kernel<double>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDerivSmemBytes));
   CK(ctx, cudaFuncSetAttribute(bssn_derivs_kernel<float>,
@@ -438,8 +443,12 @@ int b200bssn_plan_create_ex(b200bssn_ctx* ctx, const b200bssn_block* blocks, uin
     if (o.deriv_ctas_per_sm) per_sm = std::min<int>(per_sm, (int)o.deriv_ctas_per_sm);
     P->deriv_grid = std::max(1, sms * std::max(1, per_sm));
     int alg_per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&alg_per_sm, bssn_algebra_staged_kernel<RK_NONE>,
-                                                  kAlgebraThreads, kStageSmemBytes);
+    if (precision == B200BSSN_MIXED)
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&alg_per_sm, bssn_algebra_staged_kernel<float, RK_NONE>,
+                                                    StageCfg<float>::kThreads, StageCfg<float>::kSmemBytes);
+    else
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&alg_per_sm, bssn_algebra_staged_kernel<double, RK_NONE>,
+                                                    StageCfg<double>::kThreads, StageCfg<double>::kSmemBytes);
     P->alg_grid = std::max(1, sms * std::max(1, alg_per_sm));
   }
 

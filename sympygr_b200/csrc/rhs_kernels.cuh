@@ -510,10 +510,21 @@ bssn_derivs_kernel(const __grid_constant__ DerivArgs a) {
 
 constexpr size_t kDerivSmemBytes = 0;  // all shared memory is static
 
-constexpr int kStageW = 32;  // points per task of the staged algebra kernel (one warp)
-constexpr size_t kStageBytesPerWarp = (size_t)kNumDerivs * kStageW * sizeof(float) +
-                                      (size_t)kNumVars * kStageW * sizeof(double);
-constexpr size_t kStageSmemBytes = (kAlgebraThreads / 32) * kStageBytesPerWarp;  // 95,232 B
+// Staged algebra kernel geometry: 32-point tasks (one warp each); a warp's buffer
+// holds its task's 138 slot columns (FP32 or FP64) and 24 KO columns (FP64):
+// 23,808 B (MIXED) or 41,472 B (FP64).  MIXED runs 4 warps per CTA, 2 CTAs per SM
+// (the register limit of the 255-register algebra); FP64 one warp per CTA, 5 per SM
+// (the shared-memory limit).
+constexpr int kStageW = 32;
+template <typename ST>
+struct StageCfg {
+  static constexpr int kWarps = sizeof(ST) == 4 ? 4 : 1;
+  static constexpr int kThreads = 32 * kWarps;
+  static constexpr int kMinBlocks = sizeof(ST) == 4 ? 2 : 5;
+  static constexpr size_t kBytesPerWarp =
+      (size_t)kNumDerivs * kStageW * sizeof(ST) + (size_t)kNumVars * kStageW * sizeof(double);
+  static constexpr size_t kSmemBytes = kWarps * kBytesPerWarp;
+};
 
 struct AlgebraArgs {
   const double* u[kNumVars];
@@ -695,25 +706,27 @@ __device__ __forceinline__ void prefetch_l2(const void* p) {
   asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
 }
 
-// Staged algebra kernel (MIXED): persistent warps, each taking 32-point tasks
-// (quarters of a range) round-robin.  A task first copies its points' 138 FP32
-// slots and 24 KO sums into the warp's shared-memory buffer with 16-byte cp.async
-// (eight lanes per 128-byte slot column, four slots per instruction; the planner
+// Staged algebra kernel: persistent warps, each taking 32-point tasks
+// (quarters of a range) round-robin.  A task first copies its points' 138 slots
+// and 24 KO sums into the warp's shared-memory buffer with 16-byte cp.async
+// (eight or sixteen lanes per slot column; the planner
 // starts every unit's scratch run on a 32-point boundary and pads the scratch, so
 // the copies are aligned and in bounds) and prefetches the 24 state values into L2,
 // then runs the algebra reading shared memory: the loads that kept the
 // one-CTA-per-range version waiting on L2/DRAM become shared-memory loads, and while
 // one warp waits for its copies the others compute.
-template <int MODE>
-__global__ void __launch_bounds__(kAlgebraThreads, 2)
+template <typename ST, int MODE>
+__global__ void __launch_bounds__(StageCfg<ST>::kThreads, StageCfg<ST>::kMinBlocks)
 bssn_algebra_staged_kernel(const __grid_constant__ AlgebraArgs a, int ntasks) {
+  using Cfg = StageCfg<ST>;
+  using RT = ST;  // FP32 algebra in MIXED, FP64 in FP64
   extern __shared__ __align__(16) unsigned char s_stage[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  float* sd = reinterpret_cast<float*>(s_stage + warp * kStageBytesPerWarp);
-  double* sk = reinterpret_cast<double*>(s_stage + warp * kStageBytesPerWarp +
-                                         kNumDerivs * kStageW * sizeof(float));
-  const int nwarps = gridDim.x * (kAlgebraThreads / 32);
-  for (int t = blockIdx.x * (kAlgebraThreads / 32) + warp; t < ntasks; t += nwarps) {
+  ST* sd = reinterpret_cast<ST*>(s_stage + warp * Cfg::kBytesPerWarp);
+  double* sk = reinterpret_cast<double*>(s_stage + warp * Cfg::kBytesPerWarp +
+                                         kNumDerivs * kStageW * sizeof(ST));
+  const int nwarps = gridDim.x * Cfg::kWarps;
+  for (int t = blockIdx.x * Cfg::kWarps + warp; t < ntasks; t += nwarps) {
     const RangeDev rg = a.ranges[a.range_base + (t >> 2)];
     const int start = (t & 3) * kStageW;
     if (start >= rg.count) continue;
@@ -731,13 +744,15 @@ bssn_algebra_staged_kernel(const __grid_constant__ AlgebraArgs a, int ntasks) {
     }
     __syncwarp();  // every lane is done reading the previous task's buffer
     {
-      // slots: lane = 8 * (slot % 4) + chunk; chunk c holds points 4c .. 4c+3
-      const int sub = lane >> 3, c = lane & 7;
-      const float* d = static_cast<const float*>(a.dscr) + lp0 + 4 * c;
+      // a slot column is 32 * sizeof(ST) bytes = CH chunks of 16 bytes; lane =
+      // CH * (slot % (32 / CH)) + chunk
+      constexpr int CH = kStageW * (int)sizeof(ST) / 16, PER = 16 / (int)sizeof(ST);
+      const int sub = lane / CH, c = lane % CH;
+      const ST* d = static_cast<const ST*>(a.dscr) + lp0 + PER * c;
 #pragma unroll 5
-      for (int s = sub; s < kNumDerivs; s += 4)
-        cp_async16(sd + s * kStageW + 4 * c, d + (size_t)s * a.cap);
-      // KO sums: lane = 16 * (var % 2) + chunk; chunk c holds points 2c, 2c+1
+      for (int s = sub; s < kNumDerivs; s += 32 / CH)
+        cp_async16(sd + s * kStageW + PER * c, d + (size_t)s * a.cap);
+      // KO columns (FP64): lane = 16 * (var % 2) + chunk; chunk c holds points 2c, 2c+1
       const int vk = lane >> 4, ck = lane & 15;
       const double* ko = a.koscr + lp0 + 2 * ck;
 #pragma unroll 4
@@ -747,8 +762,8 @@ bssn_algebra_staged_kernel(const __grid_constant__ AlgebraArgs a, int ntasks) {
     cp_async_wait<0>();
     __syncwarp();  // the copies of every lane are visible to the whole warp
     if (valid) {
-      const SharedScratch<float> src{sd + lane, sk + lane};
-      algebra_point<float, MODE>(a, un, lpu, src);
+      const SharedScratch<ST> src{sd + lane, sk + lane};
+      algebra_point<RT, MODE>(a, un, lpu, src);
     }
   }
 }

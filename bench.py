@@ -46,8 +46,9 @@ MIXED_BAR = 1e-6
 # writes 24 x 8 B.
 SCRATCH_BYTES = {"fp64": 138 * 8 + 24 * 8, "mixed": 138 * 4 + 24 * 8}
 # DRAM bytes per interior point of each kernel measured by ncu on a large-block case
-# (profiles/ncu_derivs_algebra_large_blocks.md): derivative / algebra kernel.
-NCU_TRAFFIC_PER_POINT = {"mixed": (1242.2, 1133.9), "fp64": (1802.4, 2053.4)}
+# (profiles/ncu_derivs_algebra_large_blocks.md): derivative stage (its two kernels,
+# variables without + with second derivatives) / algebra kernel.
+NCU_TRAFFIC_PER_POINT = {"mixed": (436.0 + 672.7, 1204.6), "fp64": (597.0 + 1123.7, 1797.2)}
 
 
 def max_over_ranks(value: float, dist=None, device="cuda") -> float:
@@ -353,7 +354,7 @@ def main():
         peak_src = "measured (MEASURED_PEAKS.json hbm_gbs, copy test)"
     except Exception:
         hbm_peak, peak_src = 6650.0, "fallback 6.65 TB/s"
-    nchunks = max(1, plans[sg.MIXED].launches // 2)
+    nchunks = max(1, plans[sg.MIXED].launches // 3)  # 3 launches per chunk
 
     def hbm_roofline(kernel, ms, bytes_per_pt, mode, which):
         gbs = bytes_per_pt * npts / (ms * 1e-3) / 1e9
@@ -362,7 +363,8 @@ def main():
                 "unit": "GB/s", "frac": round(gbs / hbm_peak, 4), "traffic": round(traffic),
                 "bytes_per_point": round(bytes_per_pt, 1), "launches_per_step": nchunks,
                 "peak_source": peak_src,
-                "traffic_note": "ncu DRAM bytes/point on a 3.15M-point case x points per launch"}
+                "traffic_note": ("ncu DRAM bytes/point on a 3.15M-point case x points per chunk "
+                                 "(the derivative stage of a chunk is two launches, summed)")}
 
     # end to end through the host API: H2D of the state, evaluate, D2H of the RHS
     e2e = None
@@ -431,18 +433,18 @@ def main():
                               "per_var_rms_rel": [float(f"{x:.3g}") for x in per_var_rms]},
             "kernels_ms": {"deriv": round(d_ms, 3), "algebra": round(a_ms, 3)},
             # dominant kernel of the headline (mixed) evaluation: the derivative kernel
-            "roofline": hbm_roofline("bssn_derivs_kernel<float>", d_ms,
+            "roofline": hbm_roofline("bssn_derivs_kind_kernel<float,*> (both kinds)", d_ms,
                                      read_state + SCRATCH_BYTES["mixed"], "mixed", 0),
             "roofline_algebra": dict(
-                hbm_roofline("bssn_algebra_kernel<float,float>", a_ms,
+                hbm_roofline("bssn_algebra_staged_kernel<float,0>", a_ms,
                              24 * 8 + SCRATCH_BYTES["mixed"] + 24 * 8, "mixed", 1),
                 fp32_tflops=round(alg_tf, 3), fp32_peak=round(peak32, 2),
                 fp32_frac=round(alg_tf / peak32, 4), flops_per_point=ALGEBRA_FLOPS_PER_POINT,
                 fp_peak_source="measured FMA-chain microbenchmark (b200bssn_fma_peak)"),
             "roofline_fp64": {
-                "derivs": hbm_roofline("bssn_derivs_kernel<double>", d64,
+                "derivs": hbm_roofline("bssn_derivs_kind_kernel<double,*> (both kinds)", d64,
                                        read_state + SCRATCH_BYTES["fp64"], "fp64", 0),
-                "algebra": dict(hbm_roofline("bssn_algebra_kernel<double,double>", a64,
+                "algebra": dict(hbm_roofline("bssn_algebra_staged_kernel<double,0>", a64,
                                              24 * 8 + SCRATCH_BYTES["fp64"] + 24 * 8, "fp64", 1),
                                 fp64_tflops=round(alg64_tf, 3), fp64_peak=round(peak64, 2),
                                 fp64_frac=round(alg64_tf / peak64, 4))},

@@ -80,11 +80,22 @@ int enqueue_chunk(b200bssn_plan* P, DerivArgs da, AlgebraArgs aa, size_t ci, int
   da.koscr = P->koscr[buf];
   aa.koscr = P->koscr[buf];
   if (ev) CK(ctx, cudaEventRecord(ev[4 * ci + 0], s1));
-  dim3 g1(std::min(c.tile_count * kNumVars, P->deriv_grid), 1);
-  if (mixed)
-    bssn_derivs_kernel<float><<<g1, kDerivThreads, kDerivSmemBytes, s1>>>(da);
-  else
-    bssn_derivs_kernel<double><<<g1, kDerivThreads, kDerivSmemBytes, s1>>>(da);
+  {
+    // the two derivative kernels (variables without, then with second derivatives),
+    // each with its own work counter
+    DerivArgs dn = da, dd = da;
+    dn.counter = P->d_counters + 2 * ci;
+    dd.counter = P->d_counters + 2 * ci + 1;
+    const int gn = std::min(c.tile_count * kKindVars[0], P->deriv_grid[0]);
+    const int gd = std::min(c.tile_count * kKindVars[1], P->deriv_grid[1]);
+    if (mixed) {
+      bssn_derivs_kind_kernel<float, false><<<gn, kDerivThreads, 0, s1>>>(dn);
+      bssn_derivs_kind_kernel<float, true><<<gd, kDerivThreads, 0, s1>>>(dd);
+    } else {
+      bssn_derivs_kind_kernel<double, false><<<gn, kDerivThreads, 0, s1>>>(dn);
+      bssn_derivs_kind_kernel<double, true><<<gd, kDerivThreads, 0, s1>>>(dd);
+    }
+  }
   CK(ctx, cudaGetLastError());
   if (ev) CK(ctx, cudaEventRecord(ev[4 * ci + 1], s1));
   if (s1 != s2) {
@@ -150,7 +161,7 @@ int b200bssn::host::launch_plan(b200bssn_plan* P, double* const* rhs, const doub
   const size_t nch = P->chunks.size();
   const bool pipelined = ev == nullptr && nch > 1;
   cudaStream_t s1 = pipelined ? ctx->s_deriv : s, s2 = pipelined ? ctx->s_alg : s;
-  CK(ctx, cudaMemsetAsync(P->d_counters, 0, nch * sizeof(int), s));
+  CK(ctx, cudaMemsetAsync(P->d_counters, 0, 2 * nch * sizeof(int), s));
   if (pipelined) {
     CK(ctx, cudaEventRecord(P->ev_fork, s));
     CK(ctx, cudaStreamWaitEvent(s1, P->ev_fork, 0));
@@ -434,14 +445,19 @@ int b200bssn_plan_create_ex(b200bssn_ctx* ctx, const b200bssn_block* blocks, uin
                      [&](const TileDev& x, const TileDev& y) { return planes(x) > planes(y); });
   }
   {
-    int sms = 0, per_sm = 0;
+    int sms = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &per_sm, precision == B200BSSN_MIXED ? (const void*)bssn_derivs_kernel<float>
-                                             : (const void*)bssn_derivs_kernel<double>,
-        kDerivThreads, kDerivSmemBytes);
-    if (o.deriv_ctas_per_sm) per_sm = std::min<int>(per_sm, (int)o.deriv_ctas_per_sm);
-    P->deriv_grid = std::max(1, sms * std::max(1, per_sm));
+    const void* kinds[2] = {
+        precision == B200BSSN_MIXED ? (const void*)bssn_derivs_kind_kernel<float, false>
+                                    : (const void*)bssn_derivs_kind_kernel<double, false>,
+        precision == B200BSSN_MIXED ? (const void*)bssn_derivs_kind_kernel<float, true>
+                                    : (const void*)bssn_derivs_kind_kernel<double, true>};
+    for (int k = 0; k < 2; ++k) {
+      int per_sm = 0;
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kinds[k], kDerivThreads, 0);
+      if (o.deriv_ctas_per_sm) per_sm = std::min<int>(per_sm, (int)o.deriv_ctas_per_sm);
+      P->deriv_grid[k] = std::max(1, sms * std::max(1, per_sm));
+    }
     int alg_per_sm = 0;
     if (precision == B200BSSN_MIXED)
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&alg_per_sm, bssn_algebra_staged_kernel<float, RK_NONE>,
@@ -466,7 +482,7 @@ int b200bssn_plan_create_ex(b200bssn_ctx* ctx, const b200bssn_block* blocks, uin
     if (e == cudaSuccess) e = cudaMalloc((void**)&P->koscr[b], (size_t)kNumVars * P->cap * sizeof(double) + 512);
   }
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&P->ev_fork, cudaEventDisableTiming);
-  if (e == cudaSuccess) e = cudaMalloc((void**)&P->d_counters, P->chunks.size() * sizeof(int));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&P->d_counters, 2 * P->chunks.size() * sizeof(int));
   P->ev_deriv.assign(P->chunks.size(), nullptr);
   P->ev_alg.assign(P->chunks.size(), nullptr);
   P->ev_in.assign(P->chunks.size(), nullptr);
@@ -530,7 +546,7 @@ int b200bssn_plan_destroy(b200bssn_plan* P) {
 uint64_t b200bssn_plan_points(const b200bssn_plan* P) { return P ? P->points : 0; }
 
 uint32_t b200bssn_plan_launches(const b200bssn_plan* P) {
-  return P ? (uint32_t)(2 * P->chunks.size()) : 0;
+  return P ? (uint32_t)(3 * P->chunks.size()) : 0;  // two derivative kernels + algebra
 }
 
 int b200bssn_rhs_plan_device(b200bssn_plan* P, double* const* rhs_dev, const double* const* u_dev,
@@ -588,7 +604,7 @@ int host_pipelined(b200bssn_plan* P, double* const* rhs, const double* const* u,
   make_args(P, rd, ud, prm, da, aa);
   const size_t nch = P->chunks.size();
   cudaStream_t sin = ctx->s_h2d, s1 = ctx->s_deriv, s2 = ctx->s_alg, sout = ctx->s_d2h;
-  CK(ctx, cudaMemsetAsync(P->d_counters, 0, nch * sizeof(int), s1));
+  CK(ctx, cudaMemsetAsync(P->d_counters, 0, 2 * nch * sizeof(int), s1));
   for (size_t ci = 0; ci < nch; ++ci) {
     const uint64_t a = P->part[ci], b = P->part[ci + 1];
     const size_t nb = (size_t)(b - a) * sizeof(double);

@@ -7,7 +7,7 @@
 //   ham   = chi igt^jk R_jk - A_ij A^ij + 2/3 K^2
 //   mom_i = ...                                   (GR/constraints.py:170-177)
 // at every interior point. Here the derivatives come from the derivative kernel
-// (bssn_derivs_kernel, whose 138 slots include all 93 the constraints read), and
+// (the derivative stage, whose 138 slots include all 93 the constraints read), and
 // one thread per interior point runs the generated constraint algebra
 // (generated/bssn_constraints_algebra.cuh).
 //

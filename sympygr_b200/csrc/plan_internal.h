@@ -71,7 +71,7 @@ struct b200bssn_plan {
   bool host_pipeline = false;
   std::vector<uint64_t> part;
   std::vector<cudaEvent_t> ev_in;  // per chunk: upload done
-  int deriv_grid = 0;         // resident CTAs of the persistent derivative kernel
+  int deriv_grid[2] = {0, 0};  // resident CTAs of the two persistent derivative kernels
   int alg_grid = 0;           // resident CTAs of the persistent staged algebra kernel (MIXED)
   // host-batch staging (allocated on first host call)
   double* st_u = nullptr;

@@ -1,18 +1,26 @@
-// The two kernels of one right-hand-side evaluation of a chunk of blocks.
+// The kernels of one right-hand-side evaluation of a chunk of blocks.
 //
-//  bssn_derivs_kernel   one CTA per 16x16 column tile of a unit, streaming along
-//                       z through every variable: writes, per interior point, the
+//  derivative stage     a CTA streams one variable along z through one 16x16 column
+//                       tile of a unit and writes, per interior point, the
 //                       variable's first derivatives, its second derivatives when
 //                       it has them (mixed ones as compositions D_y(D_x u),
 //                       D_z(D_x u), D_z(D_y u), exactly as
 //                       bssn/scripts/bssnrhs_derivs.h composes them), and the sum
-//                       of its three KO terms, into the chunk's derivative scratch.
-//  bssn_algebra_kernel  one thread per interior point: the generated BSSN algebra
-//                       (or, on a flagged face plane, the Sommerfeld value of
+//                       of its three KO terms, into the chunk's derivative scratch:
+//                       bssn_derivs_kind_kernel (two persistent kernels, variables
+//                       without / with second derivatives; the plan path) or
+//                       bssn_derivs_kernel (all 24 variables; the allocation-free
+//                       entry point).
+//  algebra stage        per interior point the generated BSSN algebra (or, on a
+//                       flagged face plane, the Sommerfeld value of
 //                       bssn/src/rhs.cpp:833-977), plus sigma times the KO sum
-//                       (bssn/src/rhs.cpp:332-369), written to the RHS arrays --
-//                       or, in an RK4 stage, folded straight into the stage update
-//                       (see RkStage) so the RHS never goes to memory.
+//                       (bssn/src/rhs.cpp:332-369), written to the RHS arrays -- or,
+//                       in an RK4 stage, folded straight into the stage update (see
+//                       RkStage) so the RHS never goes to memory:
+//                       bssn_algebra_staged_kernel (persistent warps reading their
+//                       points' scratch from shared memory; the plan path) or
+//                       bssn_algebra_kernel (one CTA per 128-point run; the
+//                       allocation-free entry point).
 #pragma once
 #include <stdint.h>
 
@@ -509,6 +517,39 @@ bssn_derivs_kernel(const __grid_constant__ DerivArgs a) {
 }
 
 constexpr size_t kDerivSmemBytes = 0;  // all shared memory is static
+
+// The same items split by kind into two persistent kernels, one over the 11
+// variables with second derivatives and one over the 13 without: the latter needs
+// 80 registers instead of 128, so it runs 3 CTAs per SM instead of 2 (measured on
+// the batch: derivatives 70.0 -> 62.8 ms MIXED, 76.9 -> 71.0 ms FP64).  Plans launch
+// these; the allocation-free entry point keeps the combined kernel above.
+__device__ __forceinline__ int kind_var(bool dd, int i) {
+  constexpr int kDD[11] = {0, 1, 6, 7, 8, 12, 13, 14, 15, 16, 17};  // alpha chi beta gt
+  constexpr int kND[13] = {2, 3, 4, 5, 9, 10, 11, 18, 19, 20, 21, 22, 23};  // K Gt B At
+  return dd ? kDD[i] : kND[i];
+}
+constexpr int kKindVars[2] = {13, 11};        // [DD]
+constexpr int kKindCtasPerSm[2] = {3, 2};     // launch-bound occupancy, [DD]
+
+template <typename ST, bool DD>
+__global__ void __launch_bounds__(kDerivThreads, kKindCtasPerSm[DD])
+bssn_derivs_kind_kernel(const __grid_constant__ DerivArgs a) {
+  constexpr int NV = kKindVars[DD];
+  __shared__ double s_plane[4][kPlane];
+  __shared__ double s_dxp[DD ? 2 * kDxRows * kTileX : 1];
+  __shared__ double s_kq[(kHalo + 1) * kDerivThreads];
+  __shared__ LineScales s_sc[3];
+  __shared__ int s_item;
+  for (;;) {
+    __syncthreads();  // the previous item is finished with every shared array
+    if (threadIdx.x == 0) s_item = atomicAdd(a.counter, 1);
+    __syncthreads();
+    const int item = s_item;
+    if (item >= a.tile_count * NV) break;
+    const TileDev t = a.tiles[a.tile_base + item / NV];
+    derive_tile<ST, DD>(a, t, kind_var(DD, item % NV), s_plane, s_dxp, s_kq, s_sc);
+  }
+}
 
 // Staged algebra kernel geometry: 32-point tasks (one warp each); a warp's buffer
 // holds its task's 138 slot columns (FP32 or FP64) and 24 KO columns (FP64):

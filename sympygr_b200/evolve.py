@@ -17,7 +17,7 @@ treatment grows exponentially (its own right-hand side shows it: K grows ~2.5x e
 5 steps next to one flagged face of a 37^3 block, at any KO strength), so the
 100-step comparison runs with ``frozen``; the other two modes show that growth
 and that mixed precision follows FP64 through it.  dt = CFL * the smallest spacing.  The whole step loop runs as replays of a CUDA graph of
-``--graph-steps`` RK4 steps (each step: 4 stages x 2 launches per chunk, the stage
+``--graph-steps`` RK4 steps (each step: 4 stages x 3 launches per chunk, the stage
 update fused into the algebra kernel).  Every ``--check-every`` steps the driver
 evaluates the Hamiltonian and momentum constraints on the device (per-block sums of
 squares and maxima) and reads the lapse at the grid points nearest the two

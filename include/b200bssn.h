@@ -122,6 +122,12 @@ typedef struct b200bssn_plan_options {
   /* NULL, or one entry per block overriding slab_depth for that block (0: keep
    * slab_depth); lets a tuner pick the depth per block-size class. */
   const uint32_t *block_slab_depth;
+  /* 0: the advective terms beta^i d_i use the centred 6th-order first derivatives, as
+   * the reference's default (6th-order) build does (deriv64adv_* = deriv64_*,
+   * bssn/src/derivs.cpp:2841-2881).  1: opt-in upwind mode -- they use the 4th-order
+   * upwind stencils deriv42adv_* (bssn/src/derivs.cpp:495-900), upwinded by the sign
+   * of the matching shift component; the scratch grows by 72 slots per point. */
+  uint32_t advective;
 } b200bssn_plan_options;
 
 /* b200bssn_plan_create with explicit options (opts may be NULL). */

@@ -196,6 +196,79 @@ void bssn_oracle_ko_deriv42_z(double *Du, const double *u, double h, const unsig
   apply_axis(Du, u, sz, 2, lo, hi, &OP_KO, scales_ko(h), bflag);
 }
 
+/* ---- 4th-order upwind advective derivative, deriv42adv_x/_y/_z ---------------------
+ * bssn/src/derivs.cpp:495-900 (the upwind operator of the reference's 4th-order build;
+ * its 6th-order build wires deriv64adv_* to the centred deriv64_*, derivs.cpp:2841-2881).
+ * At interior point i of the axis, with b = beta[pp]:
+ *   centre      b > 0: (-3 u[i-1] - 10 u[i] + 18 u[i+1] - 6 u[i+2] + u[i+3]) / 12h
+ *               else : (-u[i-3] + 6 u[i-2] - 18 u[i-1] + 10 u[i] + 3 u[i+1]) / 12h
+ * and on a flagged low face (i = 3, 4, 5) / high face (i = n-6, n-5, n-4) the rows of
+ * derivs.cpp:538-575 / 577-620 (second-order one-sided or centred rows / 2h, some of
+ * them beta-dependent).  Rows are listed with offsets from i, in the reference's
+ * summation order; scales multiply the row sums. */
+typedef struct { row_t pos, neg; int half; } adv_row_t;  /* half: scale 1/2h, else 1/12h */
+
+static const row_t ADV_C_POS = {5, {{-1, -3.0}, {0, -10.0}, {1, 18.0}, {2, -6.0}, {3, 1.0}}};
+static const row_t ADV_C_NEG = {5, {{-3, -1.0}, {-2, 6.0}, {-1, -18.0}, {0, 10.0}, {1, 3.0}}};
+static const row_t ADV_FWD2 = {3, {{0, -3.0}, {1, 4.0}, {2, -1.0}}};   /* (-3,4,-1)/2h */
+static const row_t ADV_CEN2 = {2, {{-1, -1.0}, {1, 1.0}}};              /* (-1,0,1)/2h  */
+static const row_t ADV_BWD2 = {3, {{-2, 1.0}, {-1, -4.0}, {0, 3.0}}};   /* (1,-4,3)/2h  */
+
+/* low face rows i = 3, 4, 5 (derivs.cpp:538-575) and high face rows n-6, n-5, n-4
+ * (derivs.cpp:577-620); `half` marks the /2h rows of each sign */
+static const struct { const row_t *pos, *neg; int pos_half, neg_half; } ADV_LO[3] = {
+    {&ADV_FWD2, &ADV_FWD2, 1, 1},
+    {&ADV_FWD2, &ADV_CEN2, 1, 1},
+    {&ADV_C_POS, &ADV_BWD2, 0, 1},
+};
+static const struct { const row_t *pos, *neg; int pos_half, neg_half; } ADV_HI[3] = {
+    {&ADV_FWD2, &ADV_C_NEG, 1, 0},
+    {&ADV_CEN2, &ADV_BWD2, 1, 1},
+    {&ADV_BWD2, &ADV_BWD2, 1, 1},
+};
+
+static void apply_axis_adv(double *Du, const double *u, const double *beta, const unsigned int *sz,
+                           int axis, double h, unsigned int bflag) {
+  const long nx = sz[0], ny = sz[1];
+  const long stride = axis == 0 ? 1 : (axis == 1 ? nx : nx * ny);
+  const int n = (int)sz[axis];
+  const int lo_face = (bflag >> (2 * axis)) & 1u;
+  const int hi_face = (bflag >> (2 * axis + 1)) & 1u;
+  const double ih = 1.0 / h, by2 = 0.50 * ih, by12 = ih / 12.0;  /* derivs.cpp:499-501 */
+  for (int k = 3; k < (int)sz[2] - 3; ++k)
+    for (int j = 3; j < (int)sz[1] - 3; ++j)
+      for (int i = 3; i < (int)sz[0] - 3; ++i) {
+        const long pp = i + nx * (j + ny * (long)k);
+        const int pos = axis == 0 ? i : (axis == 1 ? j : k);
+        const int up = beta[pp] > 0.0;
+        const row_t *row = up ? &ADV_C_POS : &ADV_C_NEG;
+        int half = 0;
+        if (hi_face && pos >= n - 6) {
+          const int r = pos - (n - 6);
+          row = up ? ADV_HI[r].pos : ADV_HI[r].neg;
+          half = up ? ADV_HI[r].pos_half : ADV_HI[r].neg_half;
+        } else if (lo_face && pos < 6) {
+          const int r = pos - 3;
+          row = up ? ADV_LO[r].pos : ADV_LO[r].neg;
+          half = up ? ADV_LO[r].pos_half : ADV_LO[r].neg_half;
+        }
+        Du[pp] = row_sum(row, u, pp, stride) * (half ? by2 : by12);
+      }
+}
+
+void bssn_oracle_deriv42adv_x(double *Du, const double *u, double h, const unsigned int *sz,
+                              const double *beta, unsigned int bflag) {
+  apply_axis_adv(Du, u, beta, sz, 0, h, bflag);
+}
+void bssn_oracle_deriv42adv_y(double *Du, const double *u, double h, const unsigned int *sz,
+                              const double *beta, unsigned int bflag) {
+  apply_axis_adv(Du, u, beta, sz, 1, h, bflag);
+}
+void bssn_oracle_deriv42adv_z(double *Du, const double *u, double h, const unsigned int *sz,
+                              const double *beta, unsigned int bflag) {
+  apply_axis_adv(Du, u, beta, sz, 2, h, bflag);
+}
+
 /* Variables with second derivatives, in slot order (bssn/scripts/gen_bssnrhs_code:31-32),
  * given as VAR indices (bssn/include/grDef.h:31). */
 static const int DD_VAR[11] = {12, 13, 14, 15, 16, 17, 1, 0, 6, 7, 8};
@@ -262,15 +335,29 @@ static void free_arrays(double **a, int n) {
   free(a);
 }
 
-void bssn_oracle_rhs(double *const *rhs, const double *const *u, unsigned int offset,
-                     const double *pmin, const double *pmax, const unsigned int *sz,
-                     unsigned int bflag, const bssn_oracle_params *prm) {
+#define NADV (BSSN_ORACLE_NUM_DERIVS + 3 * NV)  /* derivative slots of the upwind mode */
+
+static void oracle_rhs_impl(double *const *rhs, const double *const *u, unsigned int offset,
+                            const double *pmin, const double *pmax, const unsigned int *sz,
+                            unsigned int bflag, const bssn_oracle_params *prm, int advective) {
   const int nx = (int)sz[0], ny = (int)sz[1], nz = (int)sz[2];
   const long npad = (long)nx * ny * nz;
   const double h[3] = {(pmax[0] - pmin[0]) / (nx - 1), (pmax[1] - pmin[1]) / (ny - 1),
                        (pmax[2] - pmin[2]) / (nz - 1)};
-  double **d = alloc_arrays(BSSN_ORACLE_NUM_DERIVS, npad);
+  const int nslots = advective ? NADV : BSSN_ORACLE_NUM_DERIVS;
+  double **d = alloc_arrays(nslots, npad);
   all_derivatives(d, u, offset, h, sz, bflag);
+  if (advective) {
+    /* agrad_a_<v> = adv_deriv_a(<v>, beta_a) as bssn/scripts/bssnrhs_derivs_adv.h calls it */
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int v = 0; v < NV; ++v) {
+      const double *f = u[v] + offset;
+      double **g = d + BSSN_ORACLE_NUM_DERIVS + 3 * v;
+      bssn_oracle_deriv42adv_x(g[0], f, h[0], sz, u[6] + offset, bflag);
+      bssn_oracle_deriv42adv_y(g[1], f, h[1], sz, u[7] + offset, bflag);
+      bssn_oracle_deriv42adv_z(g[2], f, h[2], sz, u[8] + offset, bflag);
+    }
+  }
 
   const double par[6] = {(double)prm->lambda[0], (double)prm->lambda[1], (double)prm->lambda[2],
                          (double)prm->lambda[3], prm->lambda_f[0],       prm->lambda_f[1]};
@@ -278,7 +365,7 @@ void bssn_oracle_rhs(double *const *rhs, const double *const *u, unsigned int of
 #pragma omp parallel for schedule(static)
   for (int k = 3; k < nz - 3; ++k) {
     const double z = pmin[2] + k * h[2];
-    double uv[NV], dv[BSSN_ORACLE_NUM_DERIVS], out[NV];
+    double uv[NV], dv[NADV], out[NV];
     for (int j = 3; j < ny - 3; ++j) {
       const double y = pmin[1] + j * h[1];
       for (int i = 3; i < nx - 3; ++i) {
@@ -288,8 +375,11 @@ void bssn_oracle_rhs(double *const *rhs, const double *const *u, unsigned int of
         double eta = prm->eta_const;
         if (r >= prm->eta_r0) eta *= pow(prm->eta_r0 / r, prm->eta_damping_exp);
         for (int v = 0; v < NV; ++v) uv[v] = u[v][offset + pp];
-        for (int s = 0; s < BSSN_ORACLE_NUM_DERIVS; ++s) dv[s] = d[s][pp];
-        bssn_oracle_algebra(uv, dv, par, eta, out);
+        for (int s = 0; s < nslots; ++s) dv[s] = d[s][pp];
+        if (advective)
+          bssn_oracle_algebra_adv(uv, dv, par, eta, out);
+        else
+          bssn_oracle_algebra(uv, dv, par, eta, out);
         for (int v = 0; v < NV; ++v) rhs[v][offset + pp] = out[v];
       }
     }
@@ -333,7 +423,19 @@ void bssn_oracle_rhs(double *const *rhs, const double *const *u, unsigned int of
         for (int v = 0; v < NV; ++v) rhs[v][offset + pp] += sigma * ko[v][pp];
       }
   free_arrays(ko, NV);
-  free_arrays(d, BSSN_ORACLE_NUM_DERIVS);
+  free_arrays(d, nslots);
+}
+
+void bssn_oracle_rhs(double *const *rhs, const double *const *u, unsigned int offset,
+                     const double *pmin, const double *pmax, const unsigned int *sz,
+                     unsigned int bflag, const bssn_oracle_params *prm) {
+  oracle_rhs_impl(rhs, u, offset, pmin, pmax, sz, bflag, prm, 0);
+}
+
+void bssn_oracle_rhs_adv(double *const *rhs, const double *const *u, unsigned int offset,
+                         const double *pmin, const double *pmax, const unsigned int *sz,
+                         unsigned int bflag, const bssn_oracle_params *prm) {
+  oracle_rhs_impl(rhs, u, offset, pmin, pmax, sz, bflag, prm, 1);
 }
 
 void bssn_oracle_derivative_slots(double *slots, const double *const *u, unsigned int offset,

@@ -41,8 +41,22 @@ void bssn_oracle_ko_deriv42_x(double *Du, const double *u, double h, const unsig
 void bssn_oracle_ko_deriv42_y(double *Du, const double *u, double h, const unsigned int *sz, unsigned int bflag);
 void bssn_oracle_ko_deriv42_z(double *Du, const double *u, double h, const unsigned int *sz, unsigned int bflag);
 
+/* 4th-order upwind advective derivatives (bssn/src/derivs.cpp:495-900): interior
+ * points only, upwinded by the sign of beta[pp] (the matching shift component). */
+void bssn_oracle_deriv42adv_x(double *Du, const double *u, double h, const unsigned int *sz,
+                              const double *beta, unsigned int bflag);
+void bssn_oracle_deriv42adv_y(double *Du, const double *u, double h, const unsigned int *sz,
+                              const double *beta, unsigned int bflag);
+void bssn_oracle_deriv42adv_z(double *Du, const double *u, double h, const unsigned int *sz,
+                              const double *beta, unsigned int bflag);
+
 /* Per-point algebra (generated; oracle/bssn_oracle_algebra.c). */
 void bssn_oracle_algebra(const double *u, const double *d, const double *par, double eta, double *out);
+
+/* The same with the advective derivatives in their own slots d[138 + 3v + a]
+ * (generated; oracle/bssn_oracle_algebra_adv.c). */
+void bssn_oracle_algebra_adv(const double *u, const double *d, const double *par, double eta,
+                             double *out);
 
 /* Per-point Hamiltonian and momentum constraints (generated;
  * oracle/bssn_oracle_constraints.c): out[4] = ham, mom0, mom1, mom2. */
@@ -60,6 +74,12 @@ void bssn_oracle_block_constraints(double *const *con, const double *const *u, u
 void bssn_oracle_rhs(double *const *rhs, const double *const *u, unsigned int offset,
                      const double *pmin, const double *pmax, const unsigned int *sz,
                      unsigned int bflag, const bssn_oracle_params *prm);
+
+/* bssn_oracle_rhs in the opt-in upwind mode: the advective terms beta^i d_i f use the
+ * 4th-order upwind derivatives above instead of the centred 6th-order ones. */
+void bssn_oracle_rhs_adv(double *const *rhs, const double *const *u, unsigned int offset,
+                         const double *pmin, const double *pmax, const unsigned int *sz,
+                         unsigned int bflag, const bssn_oracle_params *prm);
 
 /* The 162 derivative slots of one block at its interior points, compact
  * ordering p = (i-3) + I0*((j-3) + I1*(k-3)); slots[s*npts + p].  Slots

@@ -114,6 +114,43 @@ def oracle_slots(u, blk):
     return out
 
 
+def oracle_rhs_adv(u, blk, prm=None, rhs=None):
+    """The oracle's RHS in the opt-in upwind mode (advective derivatives from the
+    4th-order upwind stencils)."""
+    lib = oracle_lib()
+    u = np.ascontiguousarray(u, dtype=np.float64)
+    if rhs is None:
+        rhs = np.zeros_like(u)
+    prm = prm or params()
+    lib.bssn_oracle_rhs_adv(_ptrs(rhs), _ptrs(u), ctypes.c_uint(blk.offset), _dbl3(blk.pmin),
+                            _dbl3(blk.pmax), _uint3(blk.sz), ctypes.c_uint(blk.bflag), ctypes.byref(prm))
+    return rhs
+
+
+def _adv_call(fn, axis, f, h, sz, beta, bflag):
+    f = np.ascontiguousarray(f, dtype=np.float64)
+    beta = np.ascontiguousarray(beta, dtype=np.float64)
+    out = np.zeros_like(f)
+    args = (out.ctypes.data_as(ctypes.c_void_p), f.ctypes.data_as(ctypes.c_void_p), ctypes.c_double(h),
+            _uint3(sz), beta.ctypes.data_as(ctypes.c_void_p), ctypes.c_uint(bflag))
+    if fn is None:
+        return out, args
+    fn(*args) if axis is None else fn(ctypes.c_int(axis), *args)
+    return out
+
+
+def oracle_deriv42adv(axis, f, h, sz, beta, bflag):
+    """The oracle's upwind derivative of one padded block array along `axis`."""
+    lib = oracle_lib()
+    fn = [lib.bssn_oracle_deriv42adv_x, lib.bssn_oracle_deriv42adv_y, lib.bssn_oracle_deriv42adv_z][axis]
+    return _adv_call(fn, None, f, h, sz, beta, bflag)
+
+
+def ref_deriv42adv(axis, f, h, sz, beta, bflag, flavour="parity"):
+    """The reference's own deriv42adv_{x,y,z} (bssn/src/derivs.cpp:495-900)."""
+    return _adv_call(_ref(flavour).ref_deriv42adv, axis, f, h, sz, beta, bflag)
+
+
 def oracle_constraints(u, blk, con=None):
     """C restatement of the Hamiltonian and momentum constraints on one block:
     con[0..3] = ham, mom0, mom1, mom2 at the interior points (others untouched)."""
@@ -143,9 +180,10 @@ class OracleRK4:
     at ``init`` and updated at interior points only; the state's ghost points are
     never written).  u is [24, n_elems] float64 and is advanced in place."""
 
-    def __init__(self, blocks, n_elems, prm=None):
+    def __init__(self, blocks, n_elems, prm=None, advective=False):
         self.blocks = list(blocks)
         self.prm = prm or params()
+        self.rhs_fn = oracle_rhs_adv if advective else oracle_rhs
         self.mask = interior_elements(self.blocks, n_elems)
         self.sa = self.sb = None
 
@@ -156,7 +194,7 @@ class OracleRK4:
     def _rhs(self, state):
         r = np.zeros_like(state)
         for b in self.blocks:
-            oracle_rhs(state, b, self.prm, rhs=r)
+            self.rhs_fn(state, b, self.prm, rhs=r)
         return r[:, self.mask]
 
     def step(self, u, dt):

@@ -72,6 +72,15 @@ void ref_physical_constraints(double** con, const double** u, unsigned int offse
   physical_constraints(con, u, offset, pmin, pmax, sz, bflag);
 }
 
+// The reference's 4th-order upwind advective derivatives (bssn/src/derivs.cpp:495-900,
+// declared at bssn/include/derivs.h:23-25), for pinning the oracle's restatement.
+void ref_deriv42adv(int axis, double* Du, const double* u, double h, const unsigned int* sz,
+                    const double* beta, unsigned int bflag) {
+  if (axis == 0) deriv42adv_x(Du, u, h, sz, beta, bflag);
+  else if (axis == 1) deriv42adv_y(Du, u, h, sz, beta, bflag);
+  else deriv42adv_z(Du, u, h, sz, beta, bflag);
+}
+
 int ref_max_threads(void) { return omp_get_max_threads(); }
 
 // The reference's analytic test data (bssn/src/grUtils.cpp:15-58).

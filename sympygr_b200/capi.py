@@ -92,6 +92,7 @@ class PlanOptions(ctypes.Structure):
         ("slab_depth", ctypes.c_uint32),
         ("deriv_ctas_per_sm", ctypes.c_uint32),
         ("block_slab_depth", ctypes.POINTER(ctypes.c_uint32)),
+        ("advective", ctypes.c_uint32),
     ]
 
 
@@ -281,7 +282,7 @@ class Plan:
 
     def __init__(self, ctx: Context, blocks: Sequence[Block], precision: int = FP64,
                  chunk_points: int = 0, slab_depth: int = 0, deriv_ctas_per_sm: int = 0,
-                 block_slab_depth: Sequence[int] | None = None):
+                 block_slab_depth: Sequence[int] | None = None, advective: bool = False):
         lib = load()
         arr = (BlockC * len(blocks))()
         for i, b in enumerate(blocks):
@@ -293,6 +294,7 @@ class Plan:
             arr[i].bflag = b.bflag
         h = ctypes.c_void_p()
         opts = PlanOptions(chunk_points, slab_depth, deriv_ctas_per_sm)
+        opts.advective = 1 if advective else 0
         if block_slab_depth is not None:
             if len(block_slab_depth) != len(blocks):
                 raise ValueError("block_slab_depth needs one entry per block")

@@ -16,6 +16,7 @@ Pipeline (run where the reference tree is available; outputs are committed):
 Usage::
 
     python -m sympygr_b200.codegen.gen_bssn_rhs --reference /path/to/SymPyGR
+    python -m sympygr_b200.codegen.gen_bssn_rhs --reference /path/to/SymPyGR --advective
 """
 from __future__ import annotations
 
@@ -35,6 +36,8 @@ CUDA_OUT = os.path.join(REPO, "sympygr_b200", "csrc", "generated", "bssn_rhs_alg
 C_OUT = os.path.join(REPO, "oracle", "bssn_oracle_algebra.c")
 CUDA_CON_OUT = os.path.join(REPO, "sympygr_b200", "csrc", "generated", "bssn_constraints_algebra.cuh")
 C_CON_OUT = os.path.join(REPO, "oracle", "bssn_oracle_constraints.c")
+CUDA_ADV_OUT = os.path.join(REPO, "sympygr_b200", "csrc", "generated", "bssn_rhs_algebra_adv.cuh")
+C_ADV_OUT = os.path.join(REPO, "oracle", "bssn_oracle_algebra_adv.c")
 CON_NAMES = ["ham", "mom0", "mom1", "mom2"]
 CON_INDEX = {n: i for i, n in enumerate(CON_NAMES)}
 
@@ -273,13 +276,79 @@ void bssn_oracle_algebra(const double *u, const double *d, const double *par, do
 """
 
 
+CUDA_ADV_HEADER = """\
+// GENERATED by sympygr_b200/codegen/gen_bssn_rhs.py --advective -- do not edit by hand.
+//
+// The per-point BSSN right-hand side of bssn_rhs_algebra.cuh with the advective
+// derivatives (the beta^i d_i terms, agrad_* in GR/bssn.py) read from their own slots
+// 138..209 (agrad_<d>_<var>, VAR order, x/y/z) instead of the centred first
+// derivatives: the opt-in upwind mode, where they come from the 4th-order upwind
+// stencils (bssn/src/derivs.cpp:495-900).  Built in the same stages, %(nops)d ops,
+// %(ntmp)d temporaries.  Interface as bssn_rhs_algebra.
+#pragma once
+
+#include "bssn_rhs_algebra.cuh"
+
+namespace b200bssn {
+
+template <typename RT, class In, class Sink>
+__device__ __forceinline__ void bssn_rhs_algebra_adv(const In& in, Sink& sink,
+                                                     const AlgebraParams<RT>& prm, const RT eta) {
+"""
+
+C_ADV_HEADER = """\
+/* TEST INFRASTRUCTURE ONLY (oracle).
+ * GENERATED by sympygr_b200/codegen/gen_bssn_rhs.py --advective -- do not edit by hand.
+ *
+ * bssn_oracle_algebra with the advective derivatives in their own slots:
+ *   d[210]  d[0..137] as bssn_oracle_algebra, d[138 + 3*v + k] = agrad_k of VAR v
+ * (the beta^i d_i terms of GR/bssn.py, which the reference's default build feeds
+ * with the centred first derivatives).  %(nops)d ops after CSE.
+ */
+#include <math.h>
+#include "bssn_oracle.h"
+
+void bssn_oracle_algebra_adv(const double *u, const double *d, const double *par, double eta,
+                             double *out) {
+"""
+
+
+def main_advective(args):
+    """The upwind-mode algebra (agrad slots separate): CUDA staged + C flat."""
+    src.ADVECTIVE = True
+    slots = src.derivative_slots()[:138] + src.advective_slots()
+    CudaPrinter, CPrinter = make_printers(src.load_dendro_c_printer(args.reference))
+    t0 = time.time()
+    names, exprs = src.capture_bssn_rhs(args.reference)
+    repl, reduced = sp.cse(exprs, symbols=sp.numbered_symbols("t"), optimizations="basic")
+    print("advective: captured + cse: %.1fs, %d temporaries" % (time.time() - t0, len(repl)))
+    body, nops = emit(schedule(names, repl, reduced), CPrinter(), "c", slots)
+    with open(C_ADV_OUT, "w") as f:
+        f.write(C_ADV_HEADER % {"nops": nops})
+        f.write("\n".join(body))
+        f.write("\n}\n")
+    from .staged import capture_staged
+
+    stages = capture_staged(args.reference)
+    body, nops, ntmp = emit_staged(stages, CudaPrinter(), slots)
+    with open(CUDA_ADV_OUT, "w") as f:
+        f.write(CUDA_ADV_HEADER % {"nops": nops, "ntmp": ntmp})
+        f.write("\n".join(body))
+        f.write("\n}\n\n}  // namespace b200bssn\n")
+    print("wrote", CUDA_ADV_OUT, "and", C_ADV_OUT)
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", required=True, help="root of the SymPyGR checkout")
     ap.add_argument("--cache", default=None, help="optional pickle to reuse the CSE")
     ap.add_argument("--flat-cuda", action="store_true",
                     help="print the CUDA algebra from the single global CSE (as the C oracle)")
+    ap.add_argument("--advective", action="store_true",
+                    help="write only the upwind-mode algebra (advective derivatives in their own slots)")
     args = ap.parse_args(argv)
+    if args.advective:
+        return main_advective(args)
 
     t0 = time.time()
     if args.cache and os.path.exists(args.cache):

@@ -67,6 +67,18 @@ def derivative_slots():
     return slots
 
 
+# The advective derivatives agrad_* (bssn/scripts/bssnrhs_derivs_adv.h) are the same
+# arrays as grad_* in the reference's default 6th-order build, where deriv64adv_* is
+# deriv64_* (bssn/src/derivs.cpp:2841-2881).  With ADVECTIVE set, _rename keeps them as
+# their own symbols agrad_<d>_<var>, for the opt-in upwind mode.
+ADVECTIVE = False
+
+
+def advective_slots():
+    """The 72 advective-derivative slots of the upwind mode, VAR order, x/y/z."""
+    return [f"agrad_{d}_{v}" for v in VAR_NAMES for d in range(3)]
+
+
 def _install_import_stubs():
     """dendrosym imports tomlkit and matplotlib, neither needed for printing."""
     if "tomlkit" not in sys.modules:
@@ -167,7 +179,8 @@ def _rename(expr):
         fname = type(f).__name__
         if fname in ("grad", "agrad", "kograd"):
             d, var = f.args
-            frep[f] = sp.Symbol(f"grad_{int(d)}_{var.name}")
+            prefix = "agrad" if (fname == "agrad" and ADVECTIVE) else "grad"
+            frep[f] = sp.Symbol(f"{prefix}_{int(d)}_{var.name}")
         elif fname == "grad2":
             a, b, var = f.args
             a, b = sorted((int(a), int(b)))

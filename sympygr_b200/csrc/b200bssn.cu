@@ -35,8 +35,9 @@ bool b200bssn::host::params_ok(const b200bssn_params* p) {
 namespace {
 
 constexpr int64_t kDefaultChunkPoints = int64_t(1) << 23;
-// scratch slots are addressed with 32-bit offsets: kNumDerivs * cap < 2^31
-constexpr int64_t kMaxChunkPoints = (int64_t(1) << 31) / (kNumDerivs + 1) - 1;
+// scratch slots are addressed with 32-bit offsets: slots * cap < 2^31 (slots: 138, or
+// 210 in the upwind mode)
+constexpr int64_t max_chunk_points(int slots) { return (int64_t(1) << 31) / (slots + 1) - 1; }
 
 void make_args(const b200bssn_plan* P, double* const* rhs, const double* const* u,
                const b200bssn_params* prm, DerivArgs& da, AlgebraArgs& aa) {
@@ -60,6 +61,48 @@ void make_args(const b200bssn_plan* P, double* const* rhs, const double* const* 
   aa.eta_r0 = prm->eta_r0;
   aa.eta_damping_exp = prm->eta_damping_exp;
   aa.ko_sigma = prm->ko_sigma;
+}
+
+// The derivative stage of one chunk: the kernels over the variables without and with
+// second derivatives, each with its own work counter.
+template <typename ST, bool ADV>
+void launch_derivs(const DerivArgs& dn, const DerivArgs& dd, int gn, int gd, cudaStream_t s) {
+  bssn_derivs_kind_kernel<ST, false, ADV><<<gn, kDerivThreads, 0, s>>>(dn);
+  bssn_derivs_kind_kernel<ST, true, ADV><<<gd, kDerivThreads, 0, s>>>(dd);
+}
+
+// The staged algebra kernel for the RK mode of `aa` (RK_NONE: store the RHS).
+template <typename ST, bool ADV>
+void launch_algebra(const AlgebraArgs& aa, unsigned grid, int ntasks, cudaStream_t s) {
+  using Cfg = StageCfg<ST, ADV>;
+  switch (aa.rk.mode) {
+    case RK_FIRST:
+      bssn_algebra_staged_kernel<ST, RK_FIRST, ADV><<<grid, Cfg::kThreads, Cfg::kSmemBytes, s>>>(aa, ntasks);
+      break;
+    case RK_MIDDLE:
+      bssn_algebra_staged_kernel<ST, RK_MIDDLE, ADV><<<grid, Cfg::kThreads, Cfg::kSmemBytes, s>>>(aa, ntasks);
+      break;
+    case RK_LAST:
+      bssn_algebra_staged_kernel<ST, RK_LAST, ADV><<<grid, Cfg::kThreads, Cfg::kSmemBytes, s>>>(aa, ntasks);
+      break;
+    default:
+      bssn_algebra_staged_kernel<ST, RK_NONE, ADV><<<grid, Cfg::kThreads, Cfg::kSmemBytes, s>>>(aa, ntasks);
+      break;
+  }
+}
+
+template <typename ST, bool ADV>
+int set_stage_attributes(b200bssn_ctx* ctx) {
+  const int bytes = (int)StageCfg<ST, ADV>::kSmemBytes;
+  CK(ctx, cudaFuncSetAttribute(bssn_algebra_staged_kernel<ST, RK_NONE, ADV>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  CK(ctx, cudaFuncSetAttribute(bssn_algebra_staged_kernel<ST, RK_FIRST, ADV>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  CK(ctx, cudaFuncSetAttribute(bssn_algebra_staged_kernel<ST, RK_MIDDLE, ADV>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  CK(ctx, cudaFuncSetAttribute(bssn_algebra_staged_kernel<ST, RK_LAST, ADV>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  return B200BSSN_OK;
 }
 
 // The two kernels of chunk ci: derivatives on s1, then on s2 the algebra or, with
@@ -88,13 +131,12 @@ int enqueue_chunk(b200bssn_plan* P, DerivArgs da, AlgebraArgs aa, size_t ci, int
     dd.counter = P->d_counters + 2 * ci + 1;
     const int gn = std::min(c.tile_count * kKindVars[0], P->deriv_grid[0]);
     const int gd = std::min(c.tile_count * kKindVars[1], P->deriv_grid[1]);
-    if (mixed) {
-      bssn_derivs_kind_kernel<float, false><<<gn, kDerivThreads, 0, s1>>>(dn);
-      bssn_derivs_kind_kernel<float, true><<<gd, kDerivThreads, 0, s1>>>(dd);
-    } else {
-      bssn_derivs_kind_kernel<double, false><<<gn, kDerivThreads, 0, s1>>>(dn);
-      bssn_derivs_kind_kernel<double, true><<<gd, kDerivThreads, 0, s1>>>(dd);
-    }
+    if (mixed)
+      P->advective ? launch_derivs<float, true>(dn, dd, gn, gd, s1)
+                   : launch_derivs<float, false>(dn, dd, gn, gd, s1);
+    else
+      P->advective ? launch_derivs<double, true>(dn, dd, gn, gd, s1)
+                   : launch_derivs<double, false>(dn, dd, gn, gd, s1);
   }
   CK(ctx, cudaGetLastError());
   if (ev) CK(ctx, cudaEventRecord(ev[4 * ci + 1], s1));
@@ -112,21 +154,15 @@ int enqueue_chunk(b200bssn_plan* P, DerivArgs da, AlgebraArgs aa, size_t ci, int
     else
       bssn_constraints_kernel<double, double><<<c.range_count, kAlgebraThreads, 0, s2>>>(cc);
   } else {
+    // the staged persistent kernel: each warp takes 32-point tasks round-robin
     const int ntasks = c.range_count * (kAlgebraThreads / kStageW);
     const unsigned gs = (unsigned)std::max(1, std::min(P->alg_grid, ntasks));
-    // the staged persistent kernel: each warp takes 32-point tasks round-robin
-#define B200_ALG(MODE)                                                                          \
-  (mixed ? bssn_algebra_staged_kernel<float, MODE>                                              \
-               <<<gs, StageCfg<float>::kThreads, StageCfg<float>::kSmemBytes, s2>>>(aa, ntasks) \
-         : bssn_algebra_staged_kernel<double, MODE>                                             \
-               <<<gs, StageCfg<double>::kThreads, StageCfg<double>::kSmemBytes, s2>>>(aa, ntasks))
-    switch (aa.rk.mode) {
-      case RK_FIRST: B200_ALG(RK_FIRST); break;
-      case RK_MIDDLE: B200_ALG(RK_MIDDLE); break;
-      case RK_LAST: B200_ALG(RK_LAST); break;
-      default: B200_ALG(RK_NONE); break;
-    }
-#undef B200_ALG
+    if (mixed)
+      P->advective ? launch_algebra<float, true>(aa, gs, ntasks, s2)
+                   : launch_algebra<float, false>(aa, gs, ntasks, s2);
+    else
+      P->advective ? launch_algebra<double, true>(aa, gs, ntasks, s2)
+                   : launch_algebra<double, false>(aa, gs, ntasks, s2);
   }
   CK(ctx, cudaGetLastError());
   if (ev) CK(ctx, cudaEventRecord(ev[4 * ci + 3], s2));
@@ -179,19 +215,11 @@ int b200bssn::host::launch_plan(b200bssn_plan* P, double* const* rhs, const doub
 namespace {
 
 int set_kernel_attributes(b200bssn_ctx* ctx) {
-#define B200_STAGE_ATTR(ST, MODE)                                                        \
-  CK(ctx, cudaFuncSetAttribute(bssn_algebra_staged_kernel<ST, MODE>,                      \
-                               cudaFuncAttributeMaxDynamicSharedMemorySize,               \
-                               (int)StageCfg<ST>::kSmemBytes))
-  B200_STAGE_ATTR(float, RK_NONE);
-  B200_STAGE_ATTR(float, RK_FIRST);
-  B200_STAGE_ATTR(float, RK_MIDDLE);
-  B200_STAGE_ATTR(float, RK_LAST);
-  B200_STAGE_ATTR(double, RK_NONE);
-  B200_STAGE_ATTR(double, RK_FIRST);
-  B200_STAGE_ATTR(double, RK_MIDDLE);
-  B200_STAGE_ATTR(double, RK_LAST);
-#undef B200_STAGE_ATTR
+  int rc = set_stage_attributes<float, false>(ctx);
+  if (rc == B200BSSN_OK) rc = set_stage_attributes<float, true>(ctx);
+  if (rc == B200BSSN_OK) rc = set_stage_attributes<double, false>(ctx);
+  if (rc == B200BSSN_OK) rc = set_stage_attributes<double, true>(ctx);
+  if (rc != B200BSSN_OK) return rc;
   CK(ctx, cudaFuncSetAttribute(bssn_derivs_kernel<double>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDerivSmemBytes));
   CK(ctx, cudaFuncSetAttribute(bssn_derivs_kernel<float>,
@@ -307,6 +335,9 @@ int b200bssn_plan_create_ex(b200bssn_ctx* ctx, const b200bssn_block* blocks, uin
   b200bssn_plan* P = new b200bssn_plan();
   P->ctx = ctx;
   P->precision = precision;
+  P->advective = o.advective != 0;
+  const int nslots = P->advective ? kNumDerivs + 3 * kNumVars : kNumDerivs;
+  const int64_t kMaxChunkPoints = max_chunk_points(nslots);
   P->span_lo = UINT64_MAX;
   int64_t max_unit = 0;
   for (uint32_t b = 0; b < nblocks; ++b) {
@@ -447,11 +478,16 @@ int b200bssn_plan_create_ex(b200bssn_ctx* ctx, const b200bssn_block* blocks, uin
   {
     int sms = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
+    const bool mx = precision == B200BSSN_MIXED, adv = P->advective;
     const void* kinds[2] = {
-        precision == B200BSSN_MIXED ? (const void*)bssn_derivs_kind_kernel<float, false>
-                                    : (const void*)bssn_derivs_kind_kernel<double, false>,
-        precision == B200BSSN_MIXED ? (const void*)bssn_derivs_kind_kernel<float, true>
-                                    : (const void*)bssn_derivs_kind_kernel<double, true>};
+        mx ? (adv ? (const void*)bssn_derivs_kind_kernel<float, false, true>
+                  : (const void*)bssn_derivs_kind_kernel<float, false, false>)
+           : (adv ? (const void*)bssn_derivs_kind_kernel<double, false, true>
+                  : (const void*)bssn_derivs_kind_kernel<double, false, false>),
+        mx ? (adv ? (const void*)bssn_derivs_kind_kernel<float, true, true>
+                  : (const void*)bssn_derivs_kind_kernel<float, true, false>)
+           : (adv ? (const void*)bssn_derivs_kind_kernel<double, true, true>
+                  : (const void*)bssn_derivs_kind_kernel<double, true, false>)};
     for (int k = 0; k < 2; ++k) {
       int per_sm = 0;
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kinds[k], kDerivThreads, 0);
@@ -459,12 +495,18 @@ int b200bssn_plan_create_ex(b200bssn_ctx* ctx, const b200bssn_block* blocks, uin
       P->deriv_grid[k] = std::max(1, sms * std::max(1, per_sm));
     }
     int alg_per_sm = 0;
-    if (precision == B200BSSN_MIXED)
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&alg_per_sm, bssn_algebra_staged_kernel<float, RK_NONE>,
-                                                    StageCfg<float>::kThreads, StageCfg<float>::kSmemBytes);
+    if (mx && !adv)
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&alg_per_sm, bssn_algebra_staged_kernel<float, RK_NONE, false>,
+                                                    StageCfg<float, false>::kThreads, StageCfg<float, false>::kSmemBytes);
+    else if (mx)
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&alg_per_sm, bssn_algebra_staged_kernel<float, RK_NONE, true>,
+                                                    StageCfg<float, true>::kThreads, StageCfg<float, true>::kSmemBytes);
+    else if (!adv)
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&alg_per_sm, bssn_algebra_staged_kernel<double, RK_NONE, false>,
+                                                    StageCfg<double, false>::kThreads, StageCfg<double, false>::kSmemBytes);
     else
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&alg_per_sm, bssn_algebra_staged_kernel<double, RK_NONE>,
-                                                    StageCfg<double>::kThreads, StageCfg<double>::kSmemBytes);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&alg_per_sm, bssn_algebra_staged_kernel<double, RK_NONE, true>,
+                                                    StageCfg<double, true>::kThreads, StageCfg<double, true>::kSmemBytes);
     P->alg_grid = std::max(1, sms * std::max(1, alg_per_sm));
   }
 
@@ -478,7 +520,7 @@ int b200bssn_plan_create_ex(b200bssn_ctx* ctx, const b200bssn_block* blocks, uin
   for (int b = 0; b < nbuf && e == cudaSuccess; ++b) {
     // + 512 B: the algebra kernels' copies and prefetches of a slot run are whole
     // 16-byte chunks or 32-point columns and may read past the last run's end
-    e = cudaMalloc(&P->dscr[b], (size_t)kNumDerivs * P->cap * st + 512);
+    e = cudaMalloc(&P->dscr[b], (size_t)nslots * P->cap * st + 512);
     if (e == cudaSuccess) e = cudaMalloc((void**)&P->koscr[b], (size_t)kNumVars * P->cap * sizeof(double) + 512);
   }
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&P->ev_fork, cudaEventDisableTiming);

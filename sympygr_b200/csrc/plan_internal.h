@@ -44,6 +44,7 @@ struct ChunkRec {
 struct b200bssn_plan {
   b200bssn_ctx* ctx = nullptr;
   uint32_t precision = 0;
+  bool advective = false;  // upwind mode: 72 more scratch slots (advective derivatives)
   std::vector<BlockDev> blocks;
   std::vector<UnitDev> units;
   std::vector<TileDev> tiles;

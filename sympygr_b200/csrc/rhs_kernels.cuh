@@ -25,6 +25,7 @@
 #include <stdint.h>
 
 #include "generated/bssn_rhs_algebra.cuh"
+#include "generated/bssn_rhs_algebra_adv.cuh"
 #include "plan_types.h"
 #include "stencils.cuh"
 
@@ -230,6 +231,30 @@ struct ExactRows {
   static __device__ __forceinline__ double ko(const double (&w)[N], int C, const LineScales& c) {
     return win_ko(w, C, c);
   }
+  // upwind advective row `row` (adv_row_id) in the reference's order, each op rounded
+  template <int N>
+  static __device__ __forceinline__ D adv(const double (&w)[N], int C, int row, const LineScales& c) {
+    double a;
+    switch (row) {
+      case 0:
+        a = __dmul_rn(-3.0, w[C - 1]); a = mad_rn(a, -10.0, w[C]); a = mad_rn(a, 18.0, w[C + 1]);
+        a = mad_rn(a, -6.0, w[C + 2]); a = mad_rn(a, 1.0, w[C + 3]);
+        return __dmul_rn(a, c.d1_b);
+      case 1:
+        a = __dmul_rn(-1.0, w[C - 3]); a = mad_rn(a, 6.0, w[C - 2]); a = mad_rn(a, -18.0, w[C - 1]);
+        a = mad_rn(a, 10.0, w[C]); a = mad_rn(a, 3.0, w[C + 1]);
+        return __dmul_rn(a, c.d1_b);
+      case 2:
+        a = __dmul_rn(-3.0, w[C]); a = mad_rn(a, 4.0, w[C + 1]); a = mad_rn(a, -1.0, w[C + 2]);
+        return __dmul_rn(a, c.adv_b2);
+      case 3:
+        a = __dmul_rn(-1.0, w[C - 1]); a = mad_rn(a, 1.0, w[C + 1]);
+        return __dmul_rn(a, c.adv_b2);
+      default:
+        a = __dmul_rn(1.0, w[C - 2]); a = mad_rn(a, -4.0, w[C - 1]); a = mad_rn(a, 3.0, w[C]);
+        return __dmul_rn(a, c.adv_b2);
+    }
+  }
 };
 
 struct SplitRows {
@@ -265,6 +290,24 @@ struct SplitRows {
     const double s2 = (w[C + 2] + w[C - 2]) - u2;
     const double s3 = (w[C + 3] + w[C - 3]) - u2;
     return c.ko_c * fma(-15.0, s1, fma(6.0, s2, -s3));
+  }
+  // upwind advective rows: the weights sum to zero, so the row is a weighted sum of FP64
+  // differences from the centre value, summed in FP32
+  template <int N>
+  static __device__ __forceinline__ D adv(const double (&w)[N], int C, int row, const LineScales& c) {
+    auto dd = [&](int k) { return (float)(w[C + k] - w[C]); };
+    switch (row) {
+      case 0:
+        return fmaf(-3.0f, dd(-1), fmaf(18.0f, dd(1), fmaf(-6.0f, dd(2), dd(3)))) * (float)c.d1_b;
+      case 1:
+        return fmaf(6.0f, dd(-2), fmaf(-18.0f, dd(-1), fmaf(3.0f, dd(1), -dd(-3)))) * (float)c.d1_b;
+      case 2:
+        return fmaf(4.0f, dd(1), -dd(2)) * (float)c.adv_b2;
+      case 3:
+        return (float)(w[C + 1] - w[C - 1]) * (float)c.adv_b2;
+      default:
+        return fmaf(-4.0f, dd(-1), dd(-2)) * (float)c.adv_b2;
+    }
   }
 };
 
@@ -309,8 +352,10 @@ struct RowsFor { using type = ExactRows; };
 template <>
 struct RowsFor<float> { using type = SplitRows; };
 
-// One (column tile, variable) work item.
-template <typename ST, bool DD>
+// One (column tile, variable) work item; DD: the variable has second derivatives;
+// ADV: also the upwind advective derivatives (slots kNumDerivs + 3v + axis, upwinded
+// by the sign of the matching shift component at the point).
+template <typename ST, bool DD, bool ADV = false>
 __device__ __forceinline__ void derive_tile(const DerivArgs& a, const TileDev t, const int v,
                                             double (*s_plane)[kPlane], void* s_dxp_raw,
                                             double* s_kq, LineScales* s_sc) {
@@ -454,6 +499,15 @@ __device__ __forceinline__ void derive_tile(const DerivArgs& a, const TileDev t,
           put_slot<ST>(a, s0 + 1, lp,
                        cly ? cl_d1(pd, kTileX, gj, ny, loy, hiy, cy) : (double)Rows::d1(wd, 3, cy));
         }
+        if constexpr (ADV) {
+          // deriv42adv_x / _y (derivs.cpp:495-775) with beta0 / beta1 at the point
+          const int64_t pe = (int64_t)B.offset + gi + (int64_t)nx * gj + plane_elems * zi;
+          const bool upx = __ldg(a.u[6] + pe) > 0.0, upy = __ldg(a.u[7] + pe) > 0.0;
+          put_slot<ST>(a, kNumDerivs + 3 * v + 0, lp,
+                       (double)Rows::adv(wx, 3, adv_row_id(gi, nx, lox, hix, upx), cx));
+          put_slot<ST>(a, kNumDerivs + 3 * v + 1, lp,
+                       (double)Rows::adv(wy, 3, adv_row_id(gj, ny, loy, hiy, upy), cy));
+        }
       }
     }
     q_push(qu, u0);
@@ -481,6 +535,13 @@ __device__ __forceinline__ void derive_tile(const DerivArgs& a, const TileDev t,
         put_slot<ST>(a, s0 + 5, lp, zcl ? (double)zq_d2_closure(qu, zc, cz) : (double)Rows::d2(qu, 4, cz));
         put_slot<ST>(a, s0 + 2, lp, zcl ? (double)zq_d1_closure(qx, zc, cz) : (double)Rows::d1(qx, 4, cz));
         put_slot<ST>(a, s0 + 4, lp, zcl ? (double)zq_d1_closure(qy, zc, cz) : (double)Rows::d1(qy, 4, cz));
+      }
+      if constexpr (ADV) {
+        // deriv42adv_z (derivs.cpp:776-900) with beta2 at the point
+        const int64_t pe = (int64_t)B.offset + gi + (int64_t)nx * gj + plane_elems * zo;
+        const bool upz = __ldg(a.u[8] + pe) > 0.0;
+        put_slot<ST>(a, kNumDerivs + 3 * v + 2, lp,
+                     (double)Rows::adv(qu, 4, adv_row_id(zo, nz, loz, hiz, upz), cz));
       }
     }
   }
@@ -531,7 +592,7 @@ __device__ __forceinline__ int kind_var(bool dd, int i) {
 constexpr int kKindVars[2] = {13, 11};        // [DD]
 constexpr int kKindCtasPerSm[2] = {3, 2};     // launch-bound occupancy, [DD]
 
-template <typename ST, bool DD>
+template <typename ST, bool DD, bool ADV = false>
 __global__ void __launch_bounds__(kDerivThreads, kKindCtasPerSm[DD])
 bssn_derivs_kind_kernel(const __grid_constant__ DerivArgs a) {
   constexpr int NV = kKindVars[DD];
@@ -547,7 +608,7 @@ bssn_derivs_kind_kernel(const __grid_constant__ DerivArgs a) {
     const int item = s_item;
     if (item >= a.tile_count * NV) break;
     const TileDev t = a.tiles[a.tile_base + item / NV];
-    derive_tile<ST, DD>(a, t, kind_var(DD, item % NV), s_plane, s_dxp, s_kq, s_sc);
+    derive_tile<ST, DD, ADV>(a, t, kind_var(DD, item % NV), s_plane, s_dxp, s_kq, s_sc);
   }
 }
 
@@ -555,15 +616,17 @@ bssn_derivs_kind_kernel(const __grid_constant__ DerivArgs a) {
 // holds its task's 138 slot columns (FP32 or FP64) and 24 KO columns (FP64):
 // 23,808 B (MIXED) or 41,472 B (FP64).  MIXED runs 4 warps per CTA, 2 CTAs per SM
 // (the register limit of the 255-register algebra); FP64 one warp per CTA, 5 per SM
-// (the shared-memory limit).
+// (the shared-memory limit).  In the upwind mode (ADV) the buffer also holds the 72
+// advective-derivative columns: MIXED 2 warps per CTA, 3 CTAs per SM; FP64 3 per SM.
 constexpr int kStageW = 32;
-template <typename ST>
+template <typename ST, bool ADV = false>
 struct StageCfg {
-  static constexpr int kWarps = sizeof(ST) == 4 ? 4 : 1;
+  static constexpr int kSlots = ADV ? kNumDerivs + 3 * kNumVars : kNumDerivs;  // 210 / 138
+  static constexpr int kWarps = sizeof(ST) == 4 ? (ADV ? 2 : 4) : 1;
   static constexpr int kThreads = 32 * kWarps;
-  static constexpr int kMinBlocks = sizeof(ST) == 4 ? 2 : 5;
+  static constexpr int kMinBlocks = sizeof(ST) == 4 ? (ADV ? 3 : 2) : (ADV ? 3 : 5);
   static constexpr size_t kBytesPerWarp =
-      (size_t)kNumDerivs * kStageW * sizeof(ST) + (size_t)kNumVars * kStageW * sizeof(double);
+      (size_t)kSlots * kStageW * sizeof(ST) + (size_t)kNumVars * kStageW * sizeof(double);
   static constexpr size_t kSmemBytes = kWarps * kBytesPerWarp;
 };
 
@@ -659,7 +722,7 @@ __device__ __forceinline__ void prefetch_l2_bulk(const void* p, uint32_t bytes) 
 
 // The right-hand side of one interior point: local index lpu of unit `un`, inputs
 // through `src`.
-template <typename RT, int MODE, class Src>
+template <typename RT, int MODE, class Src, bool ADV = false>
 __device__ __forceinline__ void algebra_point(const AlgebraArgs& a, const UnitDev& un, int lpu,
                                               const Src& src) {
   const BlockDev& B = a.blocks[un.block];
@@ -703,11 +766,15 @@ __device__ __forceinline__ void algebra_point(const AlgebraArgs& a, const UnitDe
 
   PointIn<RT, Src> in{&a, pp, src};
   PointSink<MODE, Src> sink{&a, pp, src};
-  if constexpr (sizeof(RT) == 8) {
-    bssn_rhs_algebra<RT>(in, sink, a.prm64, (RT)eta);
-  } else {
-    bssn_rhs_algebra<RT>(in, sink, a.prm32, (RT)eta);
-  }
+  const AlgebraParams<RT>* prm;
+  if constexpr (sizeof(RT) == 8)
+    prm = &a.prm64;
+  else
+    prm = &a.prm32;
+  if constexpr (ADV)
+    bssn_rhs_algebra_adv<RT>(in, sink, *prm, (RT)eta);
+  else
+    bssn_rhs_algebra<RT>(in, sink, *prm, (RT)eta);
 }
 
 // One CTA per range of up to 128 consecutive points of a unit, one thread per point,
@@ -756,16 +823,16 @@ __device__ __forceinline__ void prefetch_l2(const void* p) {
 // then runs the algebra reading shared memory: the loads that kept the
 // one-CTA-per-range version waiting on L2/DRAM become shared-memory loads, and while
 // one warp waits for its copies the others compute.
-template <typename ST, int MODE>
-__global__ void __launch_bounds__(StageCfg<ST>::kThreads, StageCfg<ST>::kMinBlocks)
+template <typename ST, int MODE, bool ADV = false>
+__global__ void __launch_bounds__(StageCfg<ST, ADV>::kThreads, StageCfg<ST, ADV>::kMinBlocks)
 bssn_algebra_staged_kernel(const __grid_constant__ AlgebraArgs a, int ntasks) {
-  using Cfg = StageCfg<ST>;
+  using Cfg = StageCfg<ST, ADV>;
   using RT = ST;  // FP32 algebra in MIXED, FP64 in FP64
   extern __shared__ __align__(16) unsigned char s_stage[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   ST* sd = reinterpret_cast<ST*>(s_stage + warp * Cfg::kBytesPerWarp);
   double* sk = reinterpret_cast<double*>(s_stage + warp * Cfg::kBytesPerWarp +
-                                         kNumDerivs * kStageW * sizeof(ST));
+                                         Cfg::kSlots * kStageW * sizeof(ST));
   const int nwarps = gridDim.x * Cfg::kWarps;
   for (int t = blockIdx.x * Cfg::kWarps + warp; t < ntasks; t += nwarps) {
     const RangeDev rg = a.ranges[a.range_base + (t >> 2)];
@@ -791,7 +858,7 @@ bssn_algebra_staged_kernel(const __grid_constant__ AlgebraArgs a, int ntasks) {
       const int sub = lane / CH, c = lane % CH;
       const ST* d = static_cast<const ST*>(a.dscr) + lp0 + PER * c;
 #pragma unroll 5
-      for (int s = sub; s < kNumDerivs; s += 32 / CH)
+      for (int s = sub; s < Cfg::kSlots; s += 32 / CH)
         cp_async16(sd + s * kStageW + PER * c, d + (size_t)s * a.cap);
       // KO columns (FP64): lane = 16 * (var % 2) + chunk; chunk c holds points 2c, 2c+1
       const int vk = lane >> 4, ck = lane & 15;
@@ -804,7 +871,7 @@ bssn_algebra_staged_kernel(const __grid_constant__ AlgebraArgs a, int ntasks) {
     __syncwarp();  // the copies of every lane are visible to the whole warp
     if (valid) {
       const SharedScratch<ST> src{sd + lane, sk + lane};
-      algebra_point<RT, MODE>(a, un, lpu, src);
+      algebra_point<RT, MODE, SharedScratch<ST>, ADV>(a, un, lpu, src);
     }
   }
 }

@@ -30,6 +30,7 @@ struct LineScales {
   double d2_c, d2_b;   // idx^2/180, idx^2/12                 (derivs.cpp:2447-2449)
   double ko_c;         // -1/64/dx                            (derivs.cpp:919)
   double ko_s1, ko_s2, ko_s3;  // 49/48*64*dx, 43/48*64*dx, 59/48*64*dx (:921-923)
+  double adv_b2;       // 0.5*idx (upwind rows /2h; the /12h rows use d1_b, derivs.cpp:499-501)
 };
 
 __host__ __device__ inline LineScales make_line_scales(double h) {
@@ -44,7 +45,29 @@ __host__ __device__ inline LineScales make_line_scales(double h) {
   c.ko_s3 = 59.0 / 48.0 * 64 * h;
   c.ko_s2 = 43.0 / 48.0 * 64 * h;
   c.ko_s1 = 49.0 / 48.0 * 64 * h;
+  c.adv_b2 = 0.50 * ih;
   return c;
+}
+
+// 4th-order upwind advective derivative (bssn/src/derivs.cpp:495-900, the upwind operator
+// of the reference's 4th-order build).  Row ids, with offsets from the point in the
+// reference's summation order:
+//   0  centre, beta > 0 : (-3 u-1 - 10 u0 + 18 u1 - 6 u2 + u3) / 12h
+//   1  centre, otherwise: (-u-3 + 6 u-2 - 18 u-1 + 10 u0 + 3 u1) / 12h
+//   2  (-3 u0 + 4 u1 - u2) / 2h     3  (-u-1 + u1) / 2h     4  (u-2 - 4 u-1 + 3 u0) / 2h
+// On a flagged low face the points 3, 4, 5 use rows 2, 2|3, 0|4 (beta > 0 | otherwise;
+// derivs.cpp:538-575) and on a flagged high face the points n-6, n-5, n-4 use rows 2|1,
+// 3|4, 4 (derivs.cpp:577-620).  Every row reaches at most three points from the point.
+__host__ __device__ inline int adv_row_id(int pos, int n, bool lo, bool hi, bool up) {
+  if (hi && pos >= n - 6) {
+    const int r = pos - (n - 6);
+    return r == 0 ? (up ? 2 : 1) : (r == 1 ? (up ? 3 : 4) : 4);
+  }
+  if (lo && pos < 6) {
+    const int r = pos - 3;
+    return r == 0 ? 2 : (r == 1 ? (up ? 2 : 3) : (up ? 0 : 4));
+  }
+  return up ? 0 : 1;
 }
 
 // acc + c*v with both operations rounded separately

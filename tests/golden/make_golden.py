@@ -16,6 +16,10 @@ seeded inputs and stores its outputs:
                          (bssn/CodeGen/physcon.cpp:12)
 * con_bl_70.npz          the same on a 70^3 Brill-Lindquist block: checksums plus
                          2048 sampled interior points
+* adv42.npz              the reference's 4th-order upwind advective derivatives
+                         deriv42adv_{x,y,z} (bssn/src/derivs.cpp:495-900) of a seeded
+                         random 13x15x14 field with a seeded random shift (every 7th
+                         value exactly 0), without and with all faces flagged
 
 Each file also records the generator parameters and a SHA-256 of the input
 arrays, so a test can verify it regenerated the same inputs.
@@ -61,6 +65,20 @@ def sample_index(npts: int, seed: int) -> np.ndarray:
     return np.sort(np.random.default_rng(seed).choice(npts, NSAMPLE, replace=False))
 
 
+ADV_H = 0.07
+
+
+def adv_inputs():
+    """Seeded field and shift for the upwind-derivative fixture."""
+    sz = (13, 15, 14)
+    rng = np.random.default_rng(11)
+    n = sz[0] * sz[1] * sz[2]
+    f = rng.standard_normal(n)
+    beta = rng.standard_normal(n)
+    beta[::7] = 0.0
+    return f, beta, sz
+
+
 def main():
     if not po.have_reference("parity"):
         raise SystemExit("reference build missing: make -C oracle ref")
@@ -95,6 +113,12 @@ def main():
     np.savez_compressed(os.path.join(HERE, "con_bl_70.npz"), bflag=blk.bflag, input_sha=sha(u),
                         checksums=checksums(c), sample_index=idx, sample_con=c[:, idx])
     print("constraints bl_70", blk.sz)
+    f, beta, sz = adv_inputs()
+    outs = {f"d{axis}_b{bflag:02x}": po.ref_deriv42adv(axis, f, ADV_H, sz, beta, bflag)
+            for axis in range(3) for bflag in (0x00, 0x3F)}
+    np.savez_compressed(os.path.join(HERE, "adv42.npz"), h=ADV_H, sz=np.array(sz),
+                        input_sha=sha(np.concatenate([f, beta])), **outs)
+    print("adv42", sz)
 
 
 if __name__ == "__main__":

@@ -17,7 +17,8 @@ def algcheck(tmp_path_factory):
     exe = str(tmp_path_factory.mktemp("alg") / "algcheck")
     subprocess.run(["g++", "-O1", "-std=c++17", os.path.join(HERE, "algebra_host_check.cpp"),
                     "-x", "c", os.path.join(REPO, "oracle", "bssn_oracle_algebra.c"),
-                    os.path.join(REPO, "oracle", "bssn_oracle_constraints.c"), "-x", "none",
+                    os.path.join(REPO, "oracle", "bssn_oracle_constraints.c"),
+                    os.path.join(REPO, "oracle", "bssn_oracle_algebra_adv.c"), "-x", "none",
                     "-I", os.path.join(REPO, "sympygr_b200", "csrc", "generated"),
                     "-I", os.path.join(REPO, "oracle"), "-o", exe, "-lm"], check=True)
     return exe
@@ -38,4 +39,23 @@ def test_staged_constraint_algebra_matches_oracle(algcheck):
                          check=True).stdout
     rel = np.array([float(l.split()[1]) for l in out.strip().splitlines()])
     assert rel.shape == (4,)
+    assert rel.max() < 1e-13, rel
+
+
+def test_staged_upwind_algebra_matches_oracle(algcheck):
+    """The upwind-mode device template (advective derivatives in slots 138..209) against
+    the oracle's flat C twin."""
+    out = subprocess.run([algcheck, "3000", "adv"], capture_output=True, text=True,
+                         check=True).stdout
+    rel = np.array([float(l.split()[1]) for l in out.strip().splitlines()])
+    assert rel.shape == (24,)
+    assert rel.max() < 1e-13, rel
+
+
+def test_upwind_algebra_reduces_to_the_reference_algebra(algcheck):
+    """Fed the centred first derivatives in its advective slots, the upwind-mode algebra
+    is the reference's algebra (the oracle's, pinned to the reference)."""
+    out = subprocess.run([algcheck, "3000", "advsame"], capture_output=True, text=True,
+                         check=True).stdout
+    rel = np.array([float(l.split()[1]) for l in out.strip().splitlines()])
     assert rel.max() < 1e-13, rel

@@ -211,3 +211,51 @@ def test_oracle_rk4_is_fourth_order():
         a, b = run(dt, 1), run(dt / 2, 2)
         d.append((np.abs(a - b).max(axis=1) / np.abs(a).max(axis=1)).max())
     assert 20.0 < d[0] / d[1] < 40.0, d
+
+
+# ---- opt-in upwind mode: 4th-order upwind advective derivatives --------------------
+
+def test_oracle_upwind_derivatives_match_reference_golden(golden_dir, oracle_lib):
+    """The oracle's deriv42adv restatement against the reference's own deriv42adv_{x,y,z}
+    outputs (bitwise: same coefficients and summation order, no FMA contraction)."""
+    import importlib.util
+
+    spec = importlib.util.spec_from_file_location("make_golden", os.path.join(golden_dir, "make_golden.py"))
+    mg = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mg)
+    g = np.load(os.path.join(golden_dir, "adv42.npz"))
+    f, beta, sz = mg.adv_inputs()
+    assert _sha(np.concatenate([f, beta])) == str(g["input_sha"])
+    for axis in range(3):
+        for bflag in (0x00, 0x3F):
+            got = po.oracle_deriv42adv(axis, f, float(g["h"]), sz, beta, bflag)
+            assert np.array_equal(got, g[f"d{axis}_b{bflag:02x}"]), (axis, bflag)
+
+
+@pytest.mark.skipif(not po.have_reference("parity"), reason="reference build not present")
+@pytest.mark.parametrize("axis", [0, 1, 2])
+def test_oracle_upwind_derivatives_vs_reference_direct(oracle_lib, axis):
+    rng = np.random.default_rng(axis)
+    sz = (14, 13, 16)
+    f = rng.standard_normal(sz[0] * sz[1] * sz[2])
+    beta = rng.standard_normal(f.size)
+    for bflag in (0x00, 0x3F, 1 << (2 * axis), 2 << (2 * axis), 0x15, 0x2A):
+        a = po.oracle_deriv42adv(axis, f, 0.05, sz, beta, bflag)
+        b = po.ref_deriv42adv(axis, f, 0.05, sz, beta, bflag)
+        assert np.array_equal(a, b), bflag
+
+
+def test_oracle_upwind_rhs_differs_only_in_advection(oracle_lib):
+    """With zero shift every advective term vanishes, so the upwind-mode RHS equals the
+    standard RHS; with a shift they differ (by the advection terms only)."""
+    u, blk = po.fake_block(15, (-0.4, 0.25, -0.15), 0.06, 0x15)
+    prm = po.params(ko_sigma=0.2)
+    base = po.interior(po.oracle_rhs(u, blk, prm), blk)
+    adv = po.interior(po.oracle_rhs_adv(u, blk, prm), blk)
+    assert not np.allclose(adv, base)
+    u0 = u.copy()
+    u0[6:9] = 0.0  # beta0..2
+    a = po.interior(po.oracle_rhs(u0, blk, prm), blk)
+    b = po.interior(po.oracle_rhs_adv(u0, blk, prm), blk)
+    mx, _ = po.rel_errors(b, a)
+    assert mx.max() < 1e-13

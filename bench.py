@@ -238,6 +238,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-upwind", action="store_true", help="skip timing the opt-in upwind mode")
     ap.add_argument("--ref-fraction", type=float, default=0.0,
                     help="class-proportional block sample for the CPU reference; 0 = enough "
                          "135^3 blocks to give every host core one (min 0.1)")
@@ -335,6 +336,32 @@ def main():
         prof[prec] = (d_ms, a_ms)
     peak64 = capi.fma_peak_tflops(local_rank, sg.FP64)
     peak32 = capi.fma_peak_tflops(local_rank, sg.MIXED)
+
+    # the opt-in upwind mode (4th-order upwind advective derivatives, 72 more scratch
+    # slots) on the same batch: one plan at a time, same timing as the headline
+    upwind = None
+    if not args.no_upwind:
+        upwind = {}
+        for prec, name in ((sg.MIXED, "mixed"), (sg.FP64, "fp64")):
+            p_up = sg.Plan(ctx, blocks, prec, args.chunk_points, args.slab_depth, args.deriv_ctas,
+                           advective=True)
+            for _ in range(args.warmup):
+                p_up.rhs_device(R, U, params[prec])
+            barrier()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(args.steps):
+                p_up.rhs_device(R, U, params[prec])
+            e1.record(stream)
+            e1.synchronize()
+            ms_up = max_over_ranks(e0.elapsed_time(e1), dist) / args.steps
+            d_up, a_up = p_up.profile(R, U, params[prec])
+            p_up.close()
+            upwind[name] = {"value": round(sum_over_ranks(npts, dist) / (ms_up * 1e-3) / 1e6, 3),
+                            "ms_per_step": round(ms_up, 3), "deriv_ms": round(d_up, 3),
+                            "algebra_ms": round(a_up, 3)}
+        torch.cuda.synchronize()
 
     launches = plans[sg.MIXED].launches * args.steps
     total_pts = sum_over_ranks(npts, dist)  # each rank evaluates its own batch
@@ -448,6 +475,7 @@ def main():
                                              24 * 8 + SCRATCH_BYTES["fp64"] + 24 * 8, "fp64", 1),
                                 fp64_tflops=round(alg64_tf, 3), fp64_peak=round(peak64, 2),
                                 fp64_frac=round(alg64_tf / peak64, 4))},
+            "upwind_mode": upwind,
             "gpu_launches": launches,
             "clocks": clock_info,
             "e2e": e2e,

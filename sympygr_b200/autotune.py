@@ -9,7 +9,8 @@ for every candidate of
 * slab depth: the z-planes per work unit of the derivative kernel (candidates that
   cut the interior into the same number of slabs are the same plan, so one per
   slab count is timed);
-* derivative CTAs per SM (1 or 2 resident persistent CTAs).
+* derivative CTAs per SM: as many as fit (0; the kernel over the first-derivative-only
+  variables fits 3, the other 2) or a cap of 1 or 2 on both derivative kernels.
 
 It writes the per-class table and choice to JSON.  ``tuned_plan`` builds a plan
 for any block list from such a table: each block gets its class's slab depth
@@ -17,7 +18,7 @@ for any block list from such a table: each block gets its class's slab depth
 choice of the class holding the most points.  The run ends with the whole batch
 timed with the default knobs and with the tuned ones.
 
-    python -m sympygr_b200.autotune --precision mixed --json gpurun_out/tune_mixed.json
+    python -m sympygr_b200.autotune --precision mixed --json tune_mixed.json
 """
 from __future__ import annotations
 
@@ -86,7 +87,7 @@ def main(argv=None):
         pts = sum(b.ninterior for b in blocks)
         rows = []
         for d in depth_candidates(n):
-            for ctas in (1, 2):
+            for ctas in (0, 1, 2):
                 plan = capi.Plan(ctx, blocks, prec, slab_depth=d, deriv_ctas_per_sm=ctas)
                 ms = time_plan(plan, list(rhs), list(u), prm, args.reps)
                 plan.close()

@@ -29,7 +29,7 @@ growth over the run, the lapse history at the punctures; and, mixed against FP64
 the per-variable max and RMS relative difference of the final state's change over
 the run.
 
-    python -m sympygr_b200.evolve --steps 100 --json gpurun_out/evolve.json
+    python -m sympygr_b200.evolve --steps 100 --json evolve.json
 """
 from __future__ import annotations
 

@@ -206,3 +206,41 @@ def test_errors_are_reported(ctx):
         plan.rhs_device(list(ud), list(ud), sg.Params.make(precision=sg.MIXED))
     assert ei.value.code == -1
     plan.close()
+
+
+@pytest.mark.parametrize("sz,bflag", [((13, 21, 17), 0x00), ((19, 13, 25), 0x3F), ((23, 17, 13), 0x26)])
+def test_non_cubic_blocks_vs_oracle(ctx, oracle_lib, sz, bflag):
+    """Blocks with different extents and spacings per axis (the reference derives h per
+    axis, rhs.cpp:144-146) through the drop-in and through a plan."""
+    import torch
+
+    from sympygr_b200 import workloads as wl
+
+    pmin = (-0.37, 0.11, -0.23)
+    h = (0.031, 0.027, 0.043)
+    blk = wl.Block(5, sz, bflag, pmin, tuple(pmin[a] + (sz[a] - 1) * h[a] for a in range(3)))
+    x, y, z = wl.coords(blk)
+    u = np.zeros((24, 5 + blk.npad))
+    u[:, 5:] = po.fake_initial_data(x, y, z).reshape(24, -1)
+    ref = po.interior(po.oracle_rhs(u, blk, po.params(ko_sigma=0.3)), blk)
+    got = po.interior(_gpu_block(ctx, u, blk, 0.3), blk)
+    mx, _ = po.rel_errors(got, ref)
+    assert mx.max() < TOL64, mx.max()
+    plan = sg.Plan(ctx, [blk], sg.FP64, 600, slab_depth=4)  # 4-plane slabs over several chunks
+    assert plan.launches >= 6
+    ud = torch.from_numpy(u).cuda()
+    rd = torch.zeros_like(ud)
+    plan.rhs_device(list(rd), list(ud), sg.Params.make(ko_sigma=0.3))
+    torch.cuda.synchronize()
+    mx, _ = po.rel_errors(po.interior(rd.cpu().numpy(), blk), ref)
+    assert mx.max() < TOL64, mx.max()
+    plan.close()
+
+
+def test_plan_argument_checks(ctx):
+    u, blk = po.fake_block(13, (0.0, 0.0, 0.0), 0.1, 0)
+    for bad in ([], [wl.Block(0, (13, 13, 13), 0x40, blk.pmin, blk.pmax)],
+                [wl.Block(0, (13, 13, 13), 0, blk.pmax, blk.pmin)]):
+        with pytest.raises(sg.B200BssnError) as ei:
+            sg.Plan(ctx, bad)
+        assert ei.value.code == -1

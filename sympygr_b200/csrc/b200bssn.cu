@@ -593,6 +593,7 @@ uint32_t b200bssn_plan_launches(const b200bssn_plan* P) {
 
 int b200bssn_rhs_plan_device(b200bssn_plan* P, double* const* rhs_dev, const double* const* u_dev,
                              const b200bssn_params* prm, void* stream) {
+  b200bssn::host::NvtxRange nvtx_("b200bssn_rhs_plan_device");
   if (!P || !rhs_dev || !u_dev || !params_ok(prm)) return B200BSSN_ERR_INVALID_ARGUMENT;
   if (prm->precision != P->precision) return B200BSSN_ERR_INVALID_ARGUMENT;
   for (int v = 0; v < kNumVars; ++v)
@@ -678,6 +679,7 @@ extern "C" {
 
 int b200bssn_rhs_plan_host(b200bssn_plan* P, double* const* rhs, const double* const* u,
                            uint64_t n_elems, const b200bssn_params* prm) {
+  b200bssn::host::NvtxRange nvtx_("b200bssn_rhs_plan_host");
   if (!P || !rhs || !u || !params_ok(prm)) return B200BSSN_ERR_INVALID_ARGUMENT;
   if (prm->precision != P->precision || n_elems < P->span_hi) return B200BSSN_ERR_INVALID_ARGUMENT;
   for (int v = 0; v < kNumVars; ++v)
@@ -824,6 +826,7 @@ extern "C" {
 int b200bssn_rhs(b200bssn_ctx* ctx, double* const* rhs, const double* const* u, uint32_t offset,
                  const double* pmin, const double* pmax, const uint32_t* sz, uint32_t bflag,
                  const b200bssn_params* prm) {
+  b200bssn::host::NvtxRange nvtx_("b200bssn_rhs");
   if (!ctx || !rhs || !u || !pmin || !pmax || !sz || !params_ok(prm))
     return B200BSSN_ERR_INVALID_ARGUMENT;
   for (int v = 0; v < kNumVars; ++v)
@@ -840,6 +843,7 @@ int b200bssn_rhs(b200bssn_ctx* ctx, double* const* rhs, const double* const* u, 
 int b200bssn_physical_constraints(b200bssn_ctx* ctx, double* const* con, const double* const* u,
                                   uint32_t offset, const double* pmin, const double* pmax,
                                   const uint32_t* sz, uint32_t bflag, uint32_t precision) {
+  b200bssn::host::NvtxRange nvtx_("b200bssn_physical_constraints");
   if (!ctx || !con || !u || !pmin || !pmax || !sz) return B200BSSN_ERR_INVALID_ARGUMENT;
   if (precision != B200BSSN_FP64 && precision != B200BSSN_MIXED) return B200BSSN_ERR_INVALID_ARGUMENT;
   for (int v = 0; v < kNumVars; ++v)
@@ -862,6 +866,7 @@ int b200bssn_physical_constraints(b200bssn_ctx* ctx, double* const* con, const d
 int b200bssn_constraints_plan_device(b200bssn_plan* P, double* const* con_dev,
                                      const double* const* u_dev, double* block_norms_dev,
                                      void* stream) {
+  b200bssn::host::NvtxRange nvtx_("b200bssn_constraints_plan_device");
   if (!P || !u_dev || (!con_dev && !block_norms_dev)) return B200BSSN_ERR_INVALID_ARGUMENT;
   for (int v = 0; v < kNumVars; ++v)
     if (!u_dev[v]) return B200BSSN_ERR_INVALID_ARGUMENT;

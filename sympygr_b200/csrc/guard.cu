@@ -48,6 +48,7 @@ extern "C" {
 
 int b200bssn_check_finite(b200bssn_plan* P, const double* const* arrays, uint32_t narrays,
                           uint64_t* first_bad, void* stream) {
+  b200bssn::host::NvtxRange nvtx_("b200bssn_check_finite");
   if (!P || !arrays || narrays == 0 || narrays > (uint32_t)kNumVars) return B200BSSN_ERR_INVALID_ARGUMENT;
   for (uint32_t v = 0; v < narrays; ++v)
     if (!arrays[v]) return B200BSSN_ERR_INVALID_ARGUMENT;

@@ -3,6 +3,7 @@
 // the plan launcher the right-hand-side, constraint and RK4 entry points share.
 #pragma once
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <string>
 #include <vector>
@@ -82,6 +83,15 @@ struct b200bssn_plan {
 
 namespace b200bssn {
 namespace host {
+
+// NVTX range around an entry point (shows in Nsight Systems timelines; a no-op
+// unless a tool is attached).
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 // Records the CUDA error text on the context and maps it to a status code.
 int fail_cuda(b200bssn_ctx* ctx, cudaError_t e, const char* what);

@@ -153,6 +153,7 @@ int b200bssn_rk4_stage_state(b200bssn_rk4* R, uint32_t stage, double** state) {
 
 int b200bssn_rk4_stage(b200bssn_rk4* R, uint32_t stage, double* const* u_dev, double dt,
                        const b200bssn_params* prm, void* stream) {
+  b200bssn::host::NvtxRange nvtx_("b200bssn_rk4_stage");
   if (!step_args_ok(R, u_dev, dt, prm) || stage > 3) return B200BSSN_ERR_INVALID_ARGUMENT;
   b200bssn_ctx* ctx = R->plan->ctx;
   CK(ctx, cudaSetDevice(ctx->device));
@@ -161,6 +162,7 @@ int b200bssn_rk4_stage(b200bssn_rk4* R, uint32_t stage, double* const* u_dev, do
 
 int b200bssn_rk4_step(b200bssn_rk4* R, double* const* u_dev, double dt,
                       const b200bssn_params* prm, void* stream) {
+  b200bssn::host::NvtxRange nvtx_("b200bssn_rk4_step");
   if (!step_args_ok(R, u_dev, dt, prm)) return B200BSSN_ERR_INVALID_ARGUMENT;
   b200bssn_ctx* ctx = R->plan->ctx;
   CK(ctx, cudaSetDevice(ctx->device));
@@ -197,6 +199,7 @@ int b200bssn_rk4_graph_capture(b200bssn_rk4* R, double* const* u_dev, double dt,
 }
 
 int b200bssn_rk4_graph_launch(b200bssn_rk4* R, void* stream) {
+  b200bssn::host::NvtxRange nvtx_("b200bssn_rk4_graph_launch");
   if (!R || !R->exec) return B200BSSN_ERR_INVALID_ARGUMENT;
   b200bssn_ctx* ctx = R->plan->ctx;
   CK(ctx, cudaSetDevice(ctx->device));

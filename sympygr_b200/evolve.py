@@ -23,6 +23,10 @@ evaluates the Hamiltonian and momentum constraints on the device (per-block sums
 squares and maxima) and reads the lapse at the grid points nearest the two
 punctures.
 
+Checkpoints (``--checkpoint DIR``) are a raw dump of the final state of each run
+(``DIR/<precision>/state.npy``, [24, n] float64) with the block table, step count and
+run settings (``meta.json``); ``--resume DIR/<precision>`` continues such a run.
+
 Reported per precision: steps/s of the stepping alone and of the whole loop with
 checks, RHS evaluations per second in Mpoints/s, the constraint L2 norms and their
 growth over the run, the lapse history at the punctures; and, mixed against FP64,
@@ -81,7 +85,32 @@ def constraint_l2(norms: np.ndarray, points: int):
     return l2, mx
 
 
-def run_precision(ctx, u0, blocks, precision, args, probes, dt):
+def save_checkpoint(path: str, u, blocks, meta: dict):
+    """Raw dump of the state ([24, n] float64) plus the block table and run settings."""
+    import os
+
+    os.makedirs(path, exist_ok=True)
+    arr = u.cpu().numpy() if hasattr(u, "cpu") else np.asarray(u)
+    np.save(os.path.join(path, "state.npy"), arr)
+    meta = dict(meta)
+    meta["blocks"] = [{"offset": b.offset, "sz": list(b.sz), "bflag": b.bflag, "pmin": list(b.pmin),
+                       "pmax": list(b.pmax)} for b in blocks]
+    with open(os.path.join(path, "meta.json"), "w") as f:
+        json.dump(meta, f)
+
+
+def load_checkpoint(path: str):
+    """(state [24, n] float64, block list, settings) of a checkpoint directory."""
+    import os
+
+    with open(os.path.join(path, "meta.json")) as f:
+        meta = json.load(f)
+    blocks = [wl.Block(b["offset"], tuple(b["sz"]), b["bflag"], tuple(b["pmin"]), tuple(b["pmax"]))
+              for b in meta.pop("blocks")]
+    return np.load(os.path.join(path, "state.npy")), blocks, meta
+
+
+def run_precision(ctx, u0, blocks, precision, args, probes, dt, step0: int = 0):
     import torch
 
     plan = capi.Plan(ctx, blocks, precision, args.chunk_points)
@@ -102,7 +131,8 @@ def run_precision(ctx, u0, blocks, precision, args, probes, dt):
             nb = norms.cpu().numpy()  # ordered after the constraint kernels on ctx.stream
             lapse = u[wl.U_ALPHA].index_select(0, probe_idx).cpu().numpy()
         l2, mx = constraint_l2(nb, plan.points)
-        history.append({"step": step, "t": step * dt, "ham_l2": l2[0], "mom_l2": l2[1:].tolist(),
+        history.append({"step": step0 + step, "t": (step0 + step) * dt, "ham_l2": l2[0],
+                        "mom_l2": l2[1:].tolist(),
                         "ham_max": mx[0], "mom_max": mx[1:].tolist(), "lapse": lapse.tolist(),
                         "finite": bool(np.isfinite(nb).all())})
         return history[-1]
@@ -131,6 +161,7 @@ def run_precision(ctx, u0, blocks, precision, args, probes, dt):
                 break
     torch.cuda.synchronize()
     wall = time.perf_counter() - wall0
+    bad = plan.check_finite(cols)  # NaN/Inf guard over the final state
     final = u.cpu()  # host copy: frees HBM for the next run
     del u, cols
     rk.close()
@@ -139,6 +170,8 @@ def run_precision(ctx, u0, blocks, precision, args, probes, dt):
     return {
         "precision": "mixed" if precision == capi.MIXED else "fp64",
         "steps": done,
+        "step0": step0,
+        "finite": bad is None,
         "dt": dt,
         "graph_steps": g,
         "step_seconds": step_ms / 1e3,
@@ -165,17 +198,28 @@ def main(argv=None):
     ap.add_argument("--chunk-points", type=int, default=0)
     ap.add_argument("--precisions", default="fp64,mixed")
     ap.add_argument("--boundary", default="frozen", choices=["frozen", "batch", "all"])
+    ap.add_argument("--checkpoint", default="", help="directory for the final states")
+    ap.add_argument("--resume", default="", help="checkpoint directory of one precision to continue")
     ap.add_argument("--json", default="")
     args = ap.parse_args(argv)
 
     ctx = capi.Context(0)
-    u0, blocks = wl.two_puncture_batch_torch(wl.BATCH_SIZES, scaled_counts(args.scale), args.seed,
-                                             device="cuda")
-    if args.boundary != "batch":
-        flag = 0x3F if args.boundary == "all" else 0
-        blocks = [wl.Block(b.offset, b.sz, flag, b.pmin, b.pmax) for b in blocks]
+    step0 = 0
+    if args.resume:
+        state, blocks, meta = load_checkpoint(args.resume)
+        u0 = torch.from_numpy(state).cuda()
+        step0 = int(meta["step"])
+        dt = float(meta["dt"])
+        args.precisions = meta["precision"]
+        args.boundary = meta["boundary"]
+    else:
+        u0, blocks = wl.two_puncture_batch_torch(wl.BATCH_SIZES, scaled_counts(args.scale), args.seed,
+                                                 device="cuda")
+        if args.boundary != "batch":
+            flag = 0x3F if args.boundary == "all" else 0
+            blocks = [wl.Block(b.offset, b.sz, flag, b.pmin, b.pmax) for b in blocks]
+        dt = args.cfl * min(min(b.h) for b in blocks)
     torch.cuda.empty_cache()  # drop the initial-data temporaries before the big buffers
-    dt = args.cfl * min(min(b.h) for b in blocks)
     probes = nearest_points(blocks, PUNCTURES)
     mask = torch.zeros(u0.shape[1], dtype=torch.bool, device="cuda")
     for b in blocks:
@@ -190,9 +234,16 @@ def main(argv=None):
     finals = {}
     for name in args.precisions.split(","):
         prec = capi.MIXED if name == "mixed" else capi.FP64
-        res, fin = run_precision(ctx, u0, blocks, prec, args, probes, dt)
+        res, fin = run_precision(ctx, u0, blocks, prec, args, probes, dt, step0)
         out["runs"][name] = res
         finals[name] = fin
+        if args.checkpoint:
+            import os
+
+            save_checkpoint(os.path.join(args.checkpoint, name), fin, blocks,
+                            {"precision": name, "step": step0 + res["steps"], "dt": dt,
+                             "boundary": args.boundary, "ko_sigma": args.ko_sigma,
+                             "scale": args.scale, "seed": args.seed})
         print(json.dumps({k: v for k, v in res.items() if k != "history"}), flush=True)
     if "fp64" in finals and "mixed" in finals:
         a, b = finals["fp64"], finals["mixed"]

@@ -129,3 +129,20 @@ def test_rk4_errors_are_reported(ctx):
         assert ei.value.code == -1
     rk.close()
     plan.close()
+
+
+def test_evolve_checkpoint_resume_is_bitwise(tmp_path):
+    """4 steps straight through equal 2 steps, a checkpoint, and 2 resumed steps."""
+    from sympygr_b200 import evolve
+
+    common = ["--scale", "0.01", "--check-every", "2", "--graph-steps", "2", "--precisions", "fp64"]
+    a, b, c = (str(tmp_path / k) for k in "abc")
+    evolve.main(common + ["--steps", "4", "--checkpoint", a])
+    evolve.main(common + ["--steps", "2", "--checkpoint", b])
+    out = evolve.main(common + ["--steps", "2", "--resume", b + "/fp64", "--checkpoint", c])
+    sa, _, ma = evolve.load_checkpoint(a + "/fp64")
+    sc, _, mc = evolve.load_checkpoint(c + "/fp64")
+    assert ma["step"] == mc["step"] == 4
+    assert np.array_equal(sa, sc)
+    assert out["runs"]["fp64"]["finite"]
+    assert out["runs"]["fp64"]["history"][-1]["step"] == 4

@@ -259,3 +259,22 @@ def test_oracle_upwind_rhs_differs_only_in_advection(oracle_lib):
     b = po.interior(po.oracle_rhs_adv(u0, blk, prm), blk)
     mx, _ = po.rel_errors(b, a)
     assert mx.max() < 1e-13
+
+
+def test_oracle_is_clean_under_address_and_undefined_behaviour_sanitizers(tmp_path):
+    """The oracle's C (stencils, closures, upwind rows, algebra, constraints) built with
+    -fsanitize=address,undefined and run on one block with every face-flag pattern."""
+    import subprocess
+
+    here = os.path.dirname(os.path.abspath(__file__))
+    orc = os.path.join(os.path.dirname(here), "oracle")
+    exe = str(tmp_path / "oracle_asan")
+    srcs = [os.path.join(orc, f) for f in ("bssn_oracle.c", "bssn_oracle_algebra.c",
+                                           "bssn_oracle_algebra_adv.c", "bssn_oracle_constraints.c")]
+    subprocess.run(["gcc", "-std=c11", "-O1", "-g", "-fno-omit-frame-pointer", "-ffp-contract=off",
+                    "-fsanitize=address,undefined", "-fno-sanitize-recover=all", "-I", orc,
+                    os.path.join(here, "oracle_sanitize_main.c"), *srcs, "-o", exe, "-lm"], check=True)
+    env = dict(os.environ, ASAN_OPTIONS="detect_leaks=1", UBSAN_OPTIONS="print_stacktrace=1")
+    out = subprocess.run([exe], capture_output=True, text=True, env=env, timeout=600)
+    assert out.returncode == 0, out.stderr[-2000:]
+    assert "checksum" in out.stdout

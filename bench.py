@@ -50,6 +50,8 @@ SCRATCH_BYTES = {"fp64": 138 * 8 + 24 * 8, "mixed": 138 * 4 + 24 * 8}
 # variables without + with second derivatives) / algebra kernel.
 NCU_TRAFFIC_PER_POINT = {"mixed": (436.0 + 672.7, 1204.6), "fp64": (597.0 + 1123.7, 1797.2)}
 
+PG_TIMEOUT_S = 120  # process-group timeout under torchrun (N > 1)
+
 
 def max_over_ranks(value: float, dist=None, device="cuda") -> float:
     """The largest `value` over all ranks (every rank receives it); `dist` None: one process."""
@@ -271,7 +273,10 @@ def main():
 
         import torch.distributed as dist
 
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        # short: a rank that died leaves the others with an error at their next
+        # collective, not a wait; the longest gap between collectives (pinned staging
+        # allocation before the end-to-end timing) is well under it
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=PG_TIMEOUT_S))
 
     counts = tuple(max(1, int(round(c * args.scale))) for c in wl.BATCH_COUNTS)
     u, blocks = wl.two_puncture_batch_torch(wl.BATCH_SIZES, counts, seed=rank, device="cuda")

@@ -4,7 +4,8 @@ Each rank evaluates its own seeded batch (weak scaling, no collective on the dat
 the timing is the maximum over ranks and the point count the sum over ranks.  Here each
 rank evaluates its (small) batch through the oracle, standing in for the device work,
 and the test checks the cross-rank reductions, that the ranks' batches differ, and that
-`--impl reference` does its work on rank 0 only.
+`--impl reference` does its work on rank 0 only.  A second test has one rank raise
+between steps: the other must leave its next reduction with an error, not wait.
 """
 import datetime
 import os
@@ -63,3 +64,54 @@ def test_two_gloo_ranks_reduce_like_bench(tmp_path):
     assert r0[1] == r1[1] == r0[2] + r1[2]  # points summed over ranks
     assert r0[3] != r1[3]                   # each rank evaluated its own batch
     assert r1[4] == 0.0                     # the reference arm runs on rank 0 only
+
+
+def _failing_worker(rank, world, port, outdir, timeout_s):
+    """Rank 1 raises between steps (no collective in flight); rank 0 must leave its next
+    reduction with an error within the process-group timeout, not wait for good."""
+    import time
+
+    import torch.distributed as dist
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=timeout_s))
+    import bench
+
+    bench.max_over_ranks(1.0 + rank, dist, "cpu")  # one healthy step on both ranks
+    if rank == 1:
+        raise RuntimeError("planted failure on rank 1")
+    t0 = time.monotonic()
+    try:
+        bench.max_over_ranks(3.0, dist, "cpu")
+        status = "completed"
+    except Exception as ex:  # gloo reports the lost peer or the timeout
+        status = type(ex).__name__
+    with open(os.path.join(outdir, "r0.txt"), "w") as f:
+        f.write(f"{status} {time.monotonic() - t0:.2f}")
+
+
+def test_a_failed_rank_ends_the_others_next_reduction_with_an_error(tmp_path):
+    pytest.importorskip("torch")
+    import torch.multiprocessing as mp
+
+    timeout_s = 10
+    ctx = mp.get_context("spawn")
+    port = _free_port()
+    procs = [ctx.Process(target=_failing_worker, args=(r, 2, port, str(tmp_path), timeout_s))
+             for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=120)
+    alive = [p for p in procs if p.is_alive()]
+    for p in alive:
+        p.kill()
+        p.join()
+    assert not alive, "a rank waited past the process-group timeout"
+    assert procs[1].exitcode != 0
+    assert procs[0].exitcode == 0
+    status, secs = (tmp_path / "r0.txt").read_text().split()
+    assert status != "completed"
+    assert float(secs) < timeout_s + 30

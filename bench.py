@@ -75,6 +75,42 @@ def sum_over_ranks(value: int, dist=None, device="cuda") -> int:
     return int(t.item())
 
 
+def duplex_copy_gbs(h_src, h_dst, n: int = 128 * 1024 * 1024, reps: int = 3) -> float:
+    """GB/s per direction of a host->device and a device->host copy running at once
+    (pinned host memory, one stream per direction, `n` elements each): the transfer
+    bound of the host-buffer path, which moves its state in and its RHS out concurrently."""
+    import torch
+
+    n = min(n, h_src.numel(), h_dst.numel())
+    src, dst = h_src.view(-1)[:n], h_dst.view(-1)[:n]
+    d_in = torch.empty(n, dtype=src.dtype, device="cuda")
+    d_out = torch.zeros(n, dtype=src.dtype, device="cuda")
+    s_in, s_out = torch.cuda.Stream(), torch.cuda.Stream()
+    cur = torch.cuda.current_stream()
+
+    def once(k):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(cur)
+        s_in.wait_event(e0)
+        s_out.wait_event(e0)
+        for _ in range(k):
+            with torch.cuda.stream(s_in):
+                d_in.copy_(src, non_blocking=True)
+            with torch.cuda.stream(s_out):
+                dst.copy_(d_out, non_blocking=True)
+        cur.wait_stream(s_in)
+        cur.wait_stream(s_out)
+        e1.record(cur)
+        e1.synchronize()
+        return e0.elapsed_time(e1) * 1e-3
+
+    once(1)
+    secs = once(reps)
+    del d_in, d_out
+    return reps * n * src.element_size() / secs / 1e9
+
+
 def _env_int(k, d):
     try:
         return int(os.environ.get(k, d))
@@ -420,11 +456,20 @@ def main():
         e1.synchronize()
         ms = max_over_ranks(e0.elapsed_time(e1) / args.e2e_steps, dist)
         nbytes = 24 * span * 8
+        # the transfer bound: both directions' bytes at the concurrent copy rate
+        gbs = duplex_copy_gbs(u_h, r_h)
+        copy_ms = max_over_ranks(nbytes / (gbs * 1e9) * 1e3, dist)
         del u_h, r_h
         e2e = {"value": round(total_pts / (ms * 1e-3) / 1e6, 3), "unit": UNIT,
                "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
                "ms_per_step": round(ms, 2), "steps": args.e2e_steps,
-               "api": "b200bssn_rhs_plan_host (pinned host arrays, ghosts zeroed)"}
+               "api": "b200bssn_rhs_plan_host (pinned host arrays, ghosts zeroed)",
+               "copy_bound": {"duplex_gbs_per_direction": round(gbs, 1),
+                              "ms_per_step": round(copy_ms, 2),
+                              "value": round(total_pts / (copy_ms * 1e-3) / 1e6, 3),
+                              "frac": round(copy_ms / ms, 4),
+                              "how": "1 GiB H2D and D2H copies at once from/to the same pinned "
+                                     "arrays, one stream each; bytes per step / that rate"}}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:

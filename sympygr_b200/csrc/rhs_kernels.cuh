@@ -472,6 +472,10 @@ __device__ __forceinline__ void derive_tile(const DerivArgs& a, const TileDev t,
     if (active && in_block) {
       const double* pc = P + (ty + kHalo) * kPlaneW + (tx + kHalo);
       u0 = *pc;
+    }
+    // halo planes only feed the z queues: u for every kind, D_x u and D_y u for DD
+    if (active && in_block && (DD || out_plane)) {
+      const double* pc = P + (ty + kHalo) * kPlaneW + (tx + kHalo);
       double wx[7], wy[7];
 #pragma unroll
       for (int k = 0; k < 7; ++k) {

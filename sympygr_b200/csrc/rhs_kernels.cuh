@@ -83,6 +83,14 @@ __device__ __forceinline__ void cp_async8(double* smem_dst, const double* gmem_s
   const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem_src) : "memory");
 }
+// the copy is issued only when `p` holds; otherwise nothing is read or written
+__device__ __forceinline__ void cp_async8_if(double* smem_dst, const double* gmem_src, bool p) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
+  asm volatile(
+      "{\n .reg .pred q;\n setp.ne.b32 q, %2, 0;\n @q cp.async.ca.shared.global [%0], [%1], 8;\n}\n" ::"r"(s),
+      "l"(gmem_src), "r"((int)p)
+      : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
@@ -354,8 +362,10 @@ struct RowsFor<float> { using type = SplitRows; };
 
 // One (column tile, variable) work item; DD: the variable has second derivatives;
 // ADV: also the upwind advective derivatives (slots kNumDerivs + 3v + axis, upwinded
-// by the sign of the matching shift component at the point).
-template <typename ST, bool DD, bool ADV = false>
+// by the sign of the matching shift component at the point); CL: some point of the
+// item takes a closure row (tile_has_closure) -- without, the closure branches and
+// the face cases of the upwind rows compile away.
+template <typename ST, bool DD, bool ADV = false, bool CL = true>
 __device__ __forceinline__ void derive_tile(const DerivArgs& a, const TileDev t, const int v,
                                             double (*s_plane)[kPlane], void* s_dxp_raw,
                                             double* s_kq, LineScales* s_sc) {
@@ -371,8 +381,8 @@ __device__ __forceinline__ void derive_tile(const DerivArgs& a, const TileDev t,
   const int xlo = max(0, ox), xhi = min(nx, i0 + ex + kHalo);
   const int ylo = max(0, oy), yhi = min(ny, j0 + ey + kHalo);
   const uint32_t bf = B.bflag;
-  const bool lox = bf & 1u, hix = bf & 2u, loy = bf & 4u, hiy = bf & 8u, loz = bf & 16u,
-             hiz = bf & 32u;
+  const bool lox = CL && (bf & 1u), hix = CL && (bf & 2u), loy = CL && (bf & 4u),
+             hiy = CL && (bf & 8u), loz = CL && (bf & 16u), hiz = CL && (bf & 32u);
   if (threadIdx.x < 3) s_sc[threadIdx.x] = make_line_scales(B.h[threadIdx.x]);
 
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
@@ -417,14 +427,13 @@ __device__ __forceinline__ void derive_tile(const DerivArgs& a, const TileDev t,
 #pragma unroll
   for (int k = 0; k < kQ; ++k) qu[k] = qx[k] = qy[k] = 0.0;
 
-  // stage plane zi into buffer b (one commit group; empty past the last needed plane)
+  // stage plane zi into buffer b (one commit group; empty past the last needed plane);
+  // predicated copies, no branches
   auto stage = [&](int zi, int b) {
-    if (zi < zload) {
-      const double* fp = f + plane_elems * zi;
+    const double* fp = f + plane_elems * zi;
+    const bool in = zi < zload;
 #pragma unroll
-      for (int r = 0; r < 3; ++r)
-        if (st_ok[r]) cp_async8(&s_plane[b][st_soff[r]], fp + st_goff[r]);
-    }
+    for (int r = 0; r < 3; ++r) cp_async8_if(&s_plane[b][st_soff[r]], fp + st_goff[r], in && st_ok[r]);
     cp_async_commit();
   };
 
@@ -528,7 +537,7 @@ __device__ __forceinline__ void derive_tile(const DerivArgs& a, const TileDev t,
     const int zo = zi - kHalo;
     if (active && zo >= k0 && zo < k0 + ez) {
       const LineScales& cz = s_sc[2];
-      const int zc = z_case(zo, nz, loz, hiz);
+      const int zc = CL ? z_case(zo, nz, loz, hiz) : -1;
       const int lp = lp_col + plane_pts * (zo - k0);
       const bool zcl = zc >= 0;
       put_slot<ST>(a, 3 * v + 2, lp, zcl ? zq_d1_closure(qu, zc, cz) : (double)Rows::d1(qu, 4, cz));
@@ -550,6 +559,17 @@ __device__ __forceinline__ void derive_tile(const DerivArgs& a, const TileDev t,
     }
   }
   cp_async_wait<0>();
+}
+
+// True when some output point of the item lies within three points of a flagged
+// face (closure_row on the tile's x and y ranges or the slab's z range).
+__device__ __forceinline__ bool tile_has_closure(const DerivArgs& a, const TileDev& t) {
+  const UnitDev un = a.units[t.unit];
+  const BlockDev& B = a.blocks[un.block];
+  const uint32_t bf = B.bflag;
+  auto near = [](int p0, int e, int n, bool lo, bool hi) { return (lo && p0 < 6) || (hi && p0 + e - 1 >= n - 6); };
+  return near(3 + t.i0, t.ex, B.sz[0], bf & 1u, bf & 2u) || near(3 + t.j0, t.ey, B.sz[1], bf & 4u, bf & 8u) ||
+         near(3 + un.k0, un.nz, B.sz[2], bf & 16u, bf & 32u);
 }
 
 // Persistent derivative kernel: the grid holds as many CTAs as fit on the GPU at
@@ -574,10 +594,18 @@ bssn_derivs_kernel(const __grid_constant__ DerivArgs a) {
     // items run tile-major: the longest tiles (listed first) are all taken first
     const TileDev t = a.tiles[a.tile_base + item / kNumVars];
     const int v = item % kNumVars;
-    if (dd_index(v) >= 0)
-      derive_tile<ST, true>(a, t, v, s_plane, s_dxp, s_kq, s_sc);
-    else
-      derive_tile<ST, false>(a, t, v, s_plane, s_dxp, s_kq, s_sc);
+    const bool cl = tile_has_closure(a, t);
+    if (dd_index(v) >= 0) {
+      if (cl)
+        derive_tile<ST, true, false, true>(a, t, v, s_plane, s_dxp, s_kq, s_sc);
+      else
+        derive_tile<ST, true, false, false>(a, t, v, s_plane, s_dxp, s_kq, s_sc);
+    } else {
+      if (cl)
+        derive_tile<ST, false, false, true>(a, t, v, s_plane, s_dxp, s_kq, s_sc);
+      else
+        derive_tile<ST, false, false, false>(a, t, v, s_plane, s_dxp, s_kq, s_sc);
+    }
   }
 }
 
@@ -612,7 +640,10 @@ bssn_derivs_kind_kernel(const __grid_constant__ DerivArgs a) {
     const int item = s_item;
     if (item >= a.tile_count * NV) break;
     const TileDev t = a.tiles[a.tile_base + item / NV];
-    derive_tile<ST, DD, ADV>(a, t, kind_var(DD, item % NV), s_plane, s_dxp, s_kq, s_sc);
+    if (tile_has_closure(a, t))
+      derive_tile<ST, DD, ADV, true>(a, t, kind_var(DD, item % NV), s_plane, s_dxp, s_kq, s_sc);
+    else
+      derive_tile<ST, DD, ADV, false>(a, t, kind_var(DD, item % NV), s_plane, s_dxp, s_kq, s_sc);
   }
 }
 

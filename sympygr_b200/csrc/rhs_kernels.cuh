@@ -200,6 +200,30 @@ __device__ __forceinline__ double zq_ko_closure(const T (&q)[kQ], int zc, const 
 }
 #undef ZQ
 
+// z rows of an item on its queue q (planes zo-N/2 .. zo+N/2): with closures (CL, N =
+// kQ) the closure row `zc` where zc >= 0, else the centred row
+template <bool CL, class Rows, typename T, int N>
+__device__ __forceinline__ double zrow_d1(const T (&q)[N], int zc, const LineScales& c) {
+  if constexpr (CL) {
+    if (zc >= 0) return zq_d1_closure(q, zc, c);
+  }
+  return (double)Rows::d1(q, N / 2, c);
+}
+template <bool CL, class Rows, typename T, int N>
+__device__ __forceinline__ double zrow_d2(const T (&q)[N], int zc, const LineScales& c) {
+  if constexpr (CL) {
+    if (zc >= 0) return zq_d2_closure(q, zc, c);
+  }
+  return (double)Rows::d2(q, N / 2, c);
+}
+template <bool CL, class Rows, typename T, int N>
+__device__ __forceinline__ double zrow_ko(const T (&q)[N], int zc, const LineScales& c) {
+  if constexpr (CL) {
+    if (zc >= 0) return zq_ko_closure(q, zc, c);
+  }
+  return Rows::ko(q, N / 2, c);
+}
+
 template <typename T, int N>
 __device__ __forceinline__ void q_push(T (&q)[N], T v) {
 #pragma unroll
@@ -391,8 +415,11 @@ __device__ __forceinline__ void derive_tile(const DerivArgs& a, const TileDev t,
   // chunk-relative scratch offsets fit in 32 bits (kNumDerivs * cap < 2^31)
   const int plane_pts = I0 * I1;
   const int lp_col = (int)un.sbase + (gi - 3) + I0 * (gj - 3);  // + plane_pts * (z - k0)
-  const int zs = max(0, k0 - kHalo);
-  const int zend = k0 + ez + kHalo;  // exclusive
+  // z reach of the item's rows: closure rows reach 4 planes, centred rows 3
+  constexpr int H = CL ? kHalo : 3;
+  constexpr int QD = 2 * H + 1;
+  const int zs = max(0, k0 - H);
+  const int zend = k0 + ez + H;  // exclusive
   const int zload = min(nz, zend);   // planes beyond are never loaded
   const bool clx = closure_row(gi, nx, lox, hix), cly = closure_row(gj, ny, loy, hiy);
 
@@ -422,10 +449,10 @@ __device__ __forceinline__ void derive_tile(const DerivArgs& a, const TileDev t,
 
   const int q = DD ? dd_index(v) : -1;
   const double* __restrict__ f = a.u[v] + B.offset;
-  double qu[kQ], qx[kQ], qy[kQ];  // planes zi-8 .. zi of u, D_x u, D_y u (D_x/D_y: DD only)
-  int kslot = 0;  // ring slot of plane zi's (ko_x + ko_y) in s_kq (five planes deep)
+  double qu[QD], qx[QD], qy[QD];  // planes zi-2H .. zi of u, D_x u, D_y u (D_x/D_y: DD only)
+  int kslot = 0;  // ring slot of plane zi's (ko_x + ko_y) in s_kq (H + 1 planes deep)
 #pragma unroll
-  for (int k = 0; k < kQ; ++k) qu[k] = qx[k] = qy[k] = 0.0;
+  for (int k = 0; k < QD; ++k) qu[k] = qx[k] = qy[k] = 0.0;
 
   // stage plane zi into buffer b (one commit group; empty past the last needed plane);
   // predicated copies, no branches
@@ -528,33 +555,32 @@ __device__ __forceinline__ void derive_tile(const DerivArgs& a, const TileDev t,
       q_push(qx, dx);
       q_push(qy, dy);
     }
-    // (ko_x + ko_y) of plane zi - 4, written four steps ago into slot kslot - 4 (mod 5)
-    const int kold = kslot == kHalo ? 0 : kslot + 1;
+    // (ko_x + ko_y) of plane zi - H, written H steps ago into slot kslot - H (mod H + 1)
+    const int kold = kslot == H ? 0 : kslot + 1;
     kxy = s_kq[kold * kDerivThreads + threadIdx.x];
     kslot = kold;
 
-    // z derivatives of plane zo = zi - 4, whose +-4 neighbourhood is now queued
-    const int zo = zi - kHalo;
+    // z derivatives of plane zo = zi - H, whose +-H neighbourhood is now queued
+    const int zo = zi - H;
     if (active && zo >= k0 && zo < k0 + ez) {
       const LineScales& cz = s_sc[2];
       const int zc = CL ? z_case(zo, nz, loz, hiz) : -1;
       const int lp = lp_col + plane_pts * (zo - k0);
-      const bool zcl = zc >= 0;
-      put_slot<ST>(a, 3 * v + 2, lp, zcl ? zq_d1_closure(qu, zc, cz) : (double)Rows::d1(qu, 4, cz));
+      put_slot<ST>(a, 3 * v + 2, lp, zrow_d1<CL, Rows>(qu, zc, cz));
       // rhs.cpp:332-369 sums (ko_x + ko_y) + ko_z
-      a.koscr[v * a.cap + lp] = __dadd_rn(kxy, zcl ? zq_ko_closure(qu, zc, cz) : Rows::ko(qu, 4, cz));
+      a.koscr[v * a.cap + lp] = __dadd_rn(kxy, zrow_ko<CL, Rows>(qu, zc, cz));
       if (DD) {
         const int s0 = 72 + 6 * q;
-        put_slot<ST>(a, s0 + 5, lp, zcl ? (double)zq_d2_closure(qu, zc, cz) : (double)Rows::d2(qu, 4, cz));
-        put_slot<ST>(a, s0 + 2, lp, zcl ? (double)zq_d1_closure(qx, zc, cz) : (double)Rows::d1(qx, 4, cz));
-        put_slot<ST>(a, s0 + 4, lp, zcl ? (double)zq_d1_closure(qy, zc, cz) : (double)Rows::d1(qy, 4, cz));
+        put_slot<ST>(a, s0 + 5, lp, zrow_d2<CL, Rows>(qu, zc, cz));
+        put_slot<ST>(a, s0 + 2, lp, zrow_d1<CL, Rows>(qx, zc, cz));
+        put_slot<ST>(a, s0 + 4, lp, zrow_d1<CL, Rows>(qy, zc, cz));
       }
       if constexpr (ADV) {
         // deriv42adv_z (derivs.cpp:776-900) with beta2 at the point
         const int64_t pe = (int64_t)B.offset + gi + (int64_t)nx * gj + plane_elems * zo;
         const bool upz = __ldg(a.u[8] + pe) > 0.0;
         put_slot<ST>(a, kNumDerivs + 3 * v + 2, lp,
-                     (double)Rows::adv(qu, 4, adv_row_id(zo, nz, loz, hiz, upz), cz));
+                     (double)Rows::adv(qu, H, adv_row_id(zo, nz, loz, hiz, upz), cz));
       }
     }
   }

@@ -816,6 +816,7 @@ ConstraintArgs constraint_args(const b200bssn_plan* P, double* const* con,
   ca.units = P->d_units;
   ca.ranges = P->d_ranges;
   ca.cap = (int32_t)P->cap;
+  ca.nslots = P->advective ? kNumDerivs + 3 * kNumVars : kNumDerivs;
   return ca;
 }
 
@@ -893,21 +894,23 @@ int b200bssn_debug_block_scratch(b200bssn_ctx* ctx, double* slots, uint64_t npts
   if (P->chunks.size() != 1 || npts != P->points) return B200BSSN_ERR_INVALID_ARGUMENT;
   CK(ctx, cudaSetDevice(ctx->device));
   CK(ctx, cudaStreamSynchronize(ctx->stream));
-  std::vector<float> tmp;
-  for (int s = 0; s < kNumDerivs; ++s) {
-    if (P->precision == B200BSSN_MIXED) {
-      tmp.resize(npts);
-      CK(ctx, cudaMemcpy(tmp.data(), static_cast<float*>(P->dscr[0]) + (size_t)s * P->cap,
-                         npts * sizeof(float), cudaMemcpyDeviceToHost));
-      for (uint64_t p = 0; p < npts; ++p) slots[s * npts + p] = tmp[p];
-    } else {
-      CK(ctx, cudaMemcpy(slots + s * npts, static_cast<double*>(P->dscr[0]) + (size_t)s * P->cap,
-                         npts * sizeof(double), cudaMemcpyDeviceToHost));
-    }
+  // the scratch is blocked by 32 points (scr_index): copy it whole, then gather
+  const int ns = P->advective ? kNumDerivs + 3 * kNumVars : kNumDerivs;
+  const size_t nd = (size_t)ns * P->cap;
+  std::vector<double> d(nd), ko((size_t)kNumVars * P->cap);
+  if (P->precision == B200BSSN_MIXED) {
+    std::vector<float> tmp(nd);
+    CK(ctx, cudaMemcpy(tmp.data(), P->dscr[0], nd * sizeof(float), cudaMemcpyDeviceToHost));
+    for (size_t k = 0; k < nd; ++k) d[k] = tmp[k];
+  } else {
+    CK(ctx, cudaMemcpy(d.data(), P->dscr[0], nd * sizeof(double), cudaMemcpyDeviceToHost));
   }
+  CK(ctx, cudaMemcpy(ko.data(), P->koscr[0], ko.size() * sizeof(double), cudaMemcpyDeviceToHost));
+  auto at = [](int n, int s, uint64_t p) { return ((p >> 5) * n + s) * 32 + (p & 31); };
+  for (int s = 0; s < kNumDerivs; ++s)
+    for (uint64_t p = 0; p < npts; ++p) slots[s * npts + p] = d[at(ns, s, p)];
   for (int v = 0; v < kNumVars; ++v)
-    CK(ctx, cudaMemcpy(slots + (kNumDerivs + v) * npts, P->koscr[0] + (size_t)v * P->cap,
-                       npts * sizeof(double), cudaMemcpyDeviceToHost));
+    for (uint64_t p = 0; p < npts; ++p) slots[(kNumDerivs + v) * npts + p] = ko[at(kNumVars, v, p)];
   return B200BSSN_OK;
 }
 

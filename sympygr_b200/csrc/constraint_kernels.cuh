@@ -32,8 +32,9 @@ struct ConstraintArgs {
   const BlockDev* blocks;
   const UnitDev* units;
   const RangeDev* ranges;
-  const void* dscr;
+  const void* dscr;  // derivative slots, layout scr_index with nslots slots per point
   int32_t cap;
+  int32_t nslots;
   int32_t range_base;
 };
 
@@ -44,7 +45,7 @@ struct ConstraintIn {
   int lp;
   __device__ __forceinline__ RT u(int v) const { return (RT)__ldg(a->u[v] + pp); }
   __device__ __forceinline__ RT d(int s) const {
-    return (RT)__ldg(static_cast<const ST*>(a->dscr) + s * a->cap + lp);
+    return (RT)__ldg(static_cast<const ST*>(a->dscr) + scr_index(a->nslots, s, lp));
   }
 };
 

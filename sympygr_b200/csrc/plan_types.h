@@ -67,4 +67,18 @@ struct RkStage {
   double* base[kNumVars];  // u^n: read in every stage, written in RK_LAST
 };
 
+// Scratch layout (derivative slots and KO sums): blocks of 32 consecutive points
+// (chunk-relative index lp), each block holding its NS slots one after another --
+// value (slot s, point lp) at ((lp / 32) * NS + s) * 32 + lp % 32.  A 32-point task
+// of the algebra kernel then reads one contiguous run of NS * 32 values instead of
+// NS columns far apart (a copy of that shape reaches the full HBM read rate; 138
+// scattered 128-byte pieces per task reach about two thirds of it).
+template <int NS>
+__device__ __forceinline__ int scr_index(int s, int lp) {
+  return ((lp >> 5) * NS + s) * 32 + (lp & 31);
+}
+__device__ __forceinline__ int scr_index(int ns, int s, int lp) {
+  return ((lp >> 5) * ns + s) * 32 + (lp & 31);
+}
+
 }  // namespace b200bssn

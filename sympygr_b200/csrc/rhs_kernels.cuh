@@ -49,9 +49,9 @@ struct DerivArgs {
   const BlockDev* blocks;
   const UnitDev* units;
   const TileDev* tiles;
-  void* dscr;        // kNumDerivs slots of `cap` values (double or float)
-  double* koscr;     // kNumVars slots of `cap` doubles
-  int32_t cap;       // kNumDerivs * cap < 2^31: slots use 32-bit offsets
+  void* dscr;        // NS derivative slots (double or float), layout scr_index
+  double* koscr;     // kNumVars KO sums (double), layout scr_index
+  int32_t cap;       // points per slot (multiple of 32); NS * cap < 2^31: 32-bit offsets
   int32_t tile_base;
   int32_t tile_count;
   int* counter;      // work counter of this launch, zero at launch
@@ -95,9 +95,9 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
-template <typename ST, typename V>
+template <int NS, typename ST, typename V>
 __device__ __forceinline__ void put_slot(const DerivArgs& a, int slot, int lp, V val) {
-  static_cast<ST*>(a.dscr)[slot * a.cap + lp] = (ST)val;
+  static_cast<ST*>(a.dscr)[scr_index<NS>(slot, lp)] = (ST)val;
 }
 
 // Z-direction rows on a queue q[0..8] holding planes zo-4 .. zo+4 of one column.
@@ -394,6 +394,7 @@ __device__ __forceinline__ void derive_tile(const DerivArgs& a, const TileDev t,
                                             double (*s_plane)[kPlane], void* s_dxp_raw,
                                             double* s_kq, LineScales* s_sc) {
   using Rows = typename RowsFor<ST>::type;
+  constexpr int NS = ADV ? kNumDerivs + 3 * kNumVars : kNumDerivs;  // slots per point
   double* s_dxp = static_cast<double*>(s_dxp_raw);
   const UnitDev un = a.units[t.unit];
   const BlockDev& B = a.blocks[un.block];
@@ -526,26 +527,26 @@ __device__ __forceinline__ void derive_tile(const DerivArgs& a, const TileDev t,
         const double kx = clx ? cl_ko(pc, 1, gi, nx, lox, hix, cx) : Rows::ko(wx, 3, cx);
         const double ky = cly ? cl_ko(pc, kPlaneW, gj, ny, loy, hiy, cy) : Rows::ko(wy, 3, cy);
         s_kq[kslot * kDerivThreads + threadIdx.x] = __dadd_rn(kx, ky);
-        put_slot<ST>(a, 3 * v + 0, lp, dx);
-        put_slot<ST>(a, 3 * v + 1, lp, dy);
+        put_slot<NS, ST>(a, 3 * v + 0, lp, dx);
+        put_slot<NS, ST>(a, 3 * v + 1, lp, dy);
         if (DD) {
           const int s0 = 72 + 6 * q;
-          put_slot<ST>(a, s0 + 0, lp, clx ? cl_d2(pc, 1, gi, nx, lox, hix, cx) : (double)Rows::d2(wx, 3, cx));
-          put_slot<ST>(a, s0 + 3, lp, cly ? cl_d2(pc, kPlaneW, gj, ny, loy, hiy, cy) : (double)Rows::d2(wy, 3, cy));
+          put_slot<NS, ST>(a, s0 + 0, lp, clx ? cl_d2(pc, 1, gi, nx, lox, hix, cx) : (double)Rows::d2(wx, 3, cx));
+          put_slot<NS, ST>(a, s0 + 3, lp, cly ? cl_d2(pc, kPlaneW, gj, ny, loy, hiy, cy) : (double)Rows::d2(wy, 3, cy));
           const double* pd = Dxp + (ty + kHalo) * kTileX + tx;
           double wd[7];
 #pragma unroll
           for (int k = 0; k < 7; ++k) wd[k] = pd[(k - 3) * kTileX];
-          put_slot<ST>(a, s0 + 1, lp,
+          put_slot<NS, ST>(a, s0 + 1, lp,
                        cly ? cl_d1(pd, kTileX, gj, ny, loy, hiy, cy) : (double)Rows::d1(wd, 3, cy));
         }
         if constexpr (ADV) {
           // deriv42adv_x / _y (derivs.cpp:495-775) with beta0 / beta1 at the point
           const int64_t pe = (int64_t)B.offset + gi + (int64_t)nx * gj + plane_elems * zi;
           const bool upx = __ldg(a.u[6] + pe) > 0.0, upy = __ldg(a.u[7] + pe) > 0.0;
-          put_slot<ST>(a, kNumDerivs + 3 * v + 0, lp,
+          put_slot<NS, ST>(a, kNumDerivs + 3 * v + 0, lp,
                        (double)Rows::adv(wx, 3, adv_row_id(gi, nx, lox, hix, upx), cx));
-          put_slot<ST>(a, kNumDerivs + 3 * v + 1, lp,
+          put_slot<NS, ST>(a, kNumDerivs + 3 * v + 1, lp,
                        (double)Rows::adv(wy, 3, adv_row_id(gj, ny, loy, hiy, upy), cy));
         }
       }
@@ -566,20 +567,20 @@ __device__ __forceinline__ void derive_tile(const DerivArgs& a, const TileDev t,
       const LineScales& cz = s_sc[2];
       const int zc = CL ? z_case(zo, nz, loz, hiz) : -1;
       const int lp = lp_col + plane_pts * (zo - k0);
-      put_slot<ST>(a, 3 * v + 2, lp, zrow_d1<CL, Rows>(qu, zc, cz));
+      put_slot<NS, ST>(a, 3 * v + 2, lp, zrow_d1<CL, Rows>(qu, zc, cz));
       // rhs.cpp:332-369 sums (ko_x + ko_y) + ko_z
-      a.koscr[v * a.cap + lp] = __dadd_rn(kxy, zrow_ko<CL, Rows>(qu, zc, cz));
+      a.koscr[scr_index<kNumVars>(v, lp)] = __dadd_rn(kxy, zrow_ko<CL, Rows>(qu, zc, cz));
       if (DD) {
         const int s0 = 72 + 6 * q;
-        put_slot<ST>(a, s0 + 5, lp, zrow_d2<CL, Rows>(qu, zc, cz));
-        put_slot<ST>(a, s0 + 2, lp, zrow_d1<CL, Rows>(qx, zc, cz));
-        put_slot<ST>(a, s0 + 4, lp, zrow_d1<CL, Rows>(qy, zc, cz));
+        put_slot<NS, ST>(a, s0 + 5, lp, zrow_d2<CL, Rows>(qu, zc, cz));
+        put_slot<NS, ST>(a, s0 + 2, lp, zrow_d1<CL, Rows>(qx, zc, cz));
+        put_slot<NS, ST>(a, s0 + 4, lp, zrow_d1<CL, Rows>(qy, zc, cz));
       }
       if constexpr (ADV) {
         // deriv42adv_z (derivs.cpp:776-900) with beta2 at the point
         const int64_t pe = (int64_t)B.offset + gi + (int64_t)nx * gj + plane_elems * zo;
         const bool upz = __ldg(a.u[8] + pe) > 0.0;
-        put_slot<ST>(a, kNumDerivs + 3 * v + 2, lp,
+        put_slot<NS, ST>(a, kNumDerivs + 3 * v + 2, lp,
                      (double)Rows::adv(qu, H, adv_row_id(zo, nz, loz, hiz, upz), cz));
       }
     }
@@ -720,11 +721,10 @@ __device__ __forceinline__ double bc_asymptotic(int v) {
 // shared memory (one 32-point column per slot).
 template <typename ST>
 struct GlobalScratch {
-  const ST* d;       // dscr + lp
-  const double* ko;  // koscr + lp
-  int cap;
-  __device__ __forceinline__ ST dv(int s) const { return __ldg(d + s * cap); }
-  __device__ __forceinline__ double kov(int v) const { return __ldg(ko + v * cap); }
+  const ST* d;       // slot 0 of the point: dscr + scr_index<kNumDerivs>(0, lp)
+  const double* ko;  // koscr + scr_index<kNumVars>(0, lp)
+  __device__ __forceinline__ ST dv(int s) const { return __ldg(d + s * 32); }
+  __device__ __forceinline__ double kov(int v) const { return __ldg(ko + v * 32); }
 };
 
 template <typename ST>
@@ -845,23 +845,28 @@ __global__ void __launch_bounds__(kAlgebraThreads, 2)
 bssn_algebra_kernel(const __grid_constant__ AlgebraArgs a) {
   const RangeDev rg = a.ranges[a.range_base + blockIdx.x];
   const UnitDev un = a.units[rg.unit];
-  {
-    // pull this CTA's run of every scratch slot into L2 with one bulk prefetch per
-    // slot, so the per-point loads below hit L2 instead of waiting on DRAM
+  if (rg.count > 0) {
+    // pull this CTA's scratch into L2 first, so the per-point loads below hit L2
+    // instead of waiting on DRAM: the 32-point blocks its points fall in are one
+    // contiguous run per array (every block starts on a 16-byte boundary)
     const int lp0 = (int)un.sbase + rg.start;
-    const uint32_t bd = ((uint32_t)rg.count * (uint32_t)sizeof(ST) + 15u) & ~15u;
-    const uint32_t bk = ((uint32_t)rg.count * 8u + 15u) & ~15u;
-    for (int s = threadIdx.x; s < kNumDerivs + kNumVars; s += kAlgebraThreads) {
-      const char* p = s < kNumDerivs
-                          ? reinterpret_cast<const char*>(static_cast<const ST*>(a.dscr) + (size_t)s * a.cap + lp0)
-                          : reinterpret_cast<const char*>(a.koscr + (size_t)(s - kNumDerivs) * a.cap + lp0);
-      if ((reinterpret_cast<uintptr_t>(p) & 15u) == 0) prefetch_l2_bulk(p, s < kNumDerivs ? bd : bk);
+    const int b0 = lp0 >> 5, nblk = ((lp0 + rg.count - 1) >> 5) - b0 + 1;
+    const char* pd = reinterpret_cast<const char*>(static_cast<const ST*>(a.dscr) + (size_t)b0 * kNumDerivs * 32);
+    const char* pk = reinterpret_cast<const char*>(a.koscr + (size_t)b0 * kNumVars * 32);
+    // in pieces of at most 4 KB (both runs are multiples of 16 bytes long)
+    const uint32_t td = (uint32_t)nblk * kNumDerivs * 32 * sizeof(ST), tk = (uint32_t)nblk * kNumVars * 32 * 8;
+    const int nd = (int)((td + 4095) / 4096), nk = (int)((tk + 4095) / 4096);
+    for (int k = threadIdx.x; k < nd + nk; k += kAlgebraThreads) {
+      const bool dk = k < nd;
+      const uint32_t off = 4096u * (uint32_t)(dk ? k : k - nd), tot = dk ? td : tk;
+      prefetch_l2_bulk((dk ? pd : pk) + off, min(4096u, tot - off));
     }
   }
   if ((int)threadIdx.x >= rg.count) return;
   const int lpu = rg.start + threadIdx.x;
   const int lp = (int)un.sbase + lpu;
-  const GlobalScratch<ST> src{static_cast<const ST*>(a.dscr) + lp, a.koscr + lp, a.cap};
+  const GlobalScratch<ST> src{static_cast<const ST*>(a.dscr) + scr_index<kNumDerivs>(0, lp),
+                              a.koscr + scr_index<kNumVars>(0, lp)};
   algebra_point<RT, MODE>(a, un, lpu, src);
 }
 
@@ -913,19 +918,16 @@ bssn_algebra_staged_kernel(const __grid_constant__ AlgebraArgs a, int ntasks) {
     }
     __syncwarp();  // every lane is done reading the previous task's buffer
     {
-      // a slot column is 32 * sizeof(ST) bytes = CH chunks of 16 bytes; lane =
-      // CH * (slot % (32 / CH)) + chunk
-      constexpr int CH = kStageW * (int)sizeof(ST) / 16, PER = 16 / (int)sizeof(ST);
-      const int sub = lane / CH, c = lane % CH;
-      const ST* d = static_cast<const ST*>(a.dscr) + lp0 + PER * c;
-#pragma unroll 5
-      for (int s = sub; s < Cfg::kSlots; s += 32 / CH)
-        cp_async16(sd + s * kStageW + PER * c, d + (size_t)s * a.cap);
-      // KO columns (FP64): lane = 16 * (var % 2) + chunk; chunk c holds points 2c, 2c+1
-      const int vk = lane >> 4, ck = lane & 15;
-      const double* ko = a.koscr + lp0 + 2 * ck;
+      // the task's slots and KO sums are one contiguous block each in the scratch
+      // (scr_index; lp0 is a multiple of 32), laid out exactly as the buffer wants
+      // them: copy both in 16-byte pieces, lane-strided
+      constexpr int ND = Cfg::kSlots * kStageW * (int)sizeof(ST) / 16, NK = kNumVars * kStageW * 8 / 16;
+      const char* d = reinterpret_cast<const char*>(static_cast<const ST*>(a.dscr) + (size_t)lp0 * Cfg::kSlots);
+      const char* ko = reinterpret_cast<const char*>(a.koscr + (size_t)lp0 * kNumVars);
+#pragma unroll 6
+      for (int k = lane; k < ND; k += 32) cp_async16(reinterpret_cast<char*>(sd) + 16 * k, d + 16 * k);
 #pragma unroll 4
-      for (int v = vk; v < kNumVars; v += 2) cp_async16(sk + v * kStageW + 2 * ck, ko + (size_t)v * a.cap);
+      for (int k = lane; k < NK; k += 32) cp_async16(reinterpret_cast<char*>(sk) + 16 * k, ko + 16 * k);
     }
     cp_async_commit();
     cp_async_wait<0>();

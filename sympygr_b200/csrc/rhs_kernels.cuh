@@ -66,11 +66,13 @@ struct DerivArgs {
 // (cp.async into four plane buffers: three planes stream in while one is
 // differentiated).  In-plane derivatives (D_x, D_y, D_xx, D_yy, D_y(D_x), ko_x,
 // ko_y) come from that plane; the z derivatives of the variable and of its D_x
-// and D_y (D_z, D_zz, ko_z, D_z(D_x), D_z(D_y)) come from 9-deep register queues
-// that each thread keeps for its own column, so every plane is loaded once per
-// variable and no z halo is recomputed.  The item's code is instantiated twice,
-// for variables with and without second derivatives (DD), so the 13 variables
-// that need only first derivatives and KO carry no D_x/D_y queues or halo rows.
+// and D_y (D_z, D_zz, ko_z, D_z(D_x), D_z(D_y)) come from register queues that
+// each thread keeps for its own column (9 planes deep where a closure row may reach
+// 4 planes, else 7), so every plane is loaded once per variable and no z halo is
+// recomputed.  The item's code is instantiated for variables with and without
+// second derivatives (DD), so the 13 variables that need only first derivatives and
+// KO carry no D_x/D_y queues or halo rows, and for items with and without closure
+// rows (CL), so the items away from flagged faces carry no closure tests.
 // ---------------------------------------------------------------------------
 constexpr int kPlaneW = kTileX + 2 * kHalo;  // 24: plane width incl. halo
 constexpr int kPlaneH = kTileY + 2 * kHalo;  // 24
@@ -413,7 +415,7 @@ __device__ __forceinline__ void derive_tile(const DerivArgs& a, const TileDev t,
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
   const bool active = tx < ex && ty < ey;
   const int gi = i0 + tx, gj = j0 + ty;
-  // chunk-relative scratch offsets fit in 32 bits (kNumDerivs * cap < 2^31)
+  // chunk-relative scratch offsets fit in 32 bits (NS * cap < 2^31)
   const int plane_pts = I0 * I1;
   const int lp_col = (int)un.sbase + (gi - 3) + I0 * (gj - 3);  // + plane_pts * (z - k0)
   // z reach of the item's rows: closure rows reach 4 planes, centred rows 3
@@ -675,7 +677,8 @@ bssn_derivs_kind_kernel(const __grid_constant__ DerivArgs a) {
 }
 
 // Staged algebra kernel geometry: 32-point tasks (one warp each); a warp's buffer
-// holds its task's 138 slot columns (FP32 or FP64) and 24 KO columns (FP64):
+// holds its task's 138 slots (FP32 or FP64) and 24 KO sums (FP64) per point, laid
+// out as the blocked scratch holds them (scr_index):
 // 23,808 B (MIXED) or 41,472 B (FP64).  MIXED runs 4 warps per CTA, 2 CTAs per SM
 // (the register limit of the 255-register algebra); FP64 one warp per CTA, 5 per SM
 // (the shared-memory limit).  In the upwind mode (ADV) the buffer also holds the 72
@@ -882,8 +885,8 @@ __device__ __forceinline__ void prefetch_l2(const void* p) {
 
 // Staged algebra kernel: persistent warps, each taking 32-point tasks
 // (quarters of a range) round-robin.  A task first copies its points' 138 slots
-// and 24 KO sums into the warp's shared-memory buffer with 16-byte cp.async
-// (eight or sixteen lanes per slot column; the planner
+// and 24 KO sums -- one contiguous block each in the blocked scratch -- into the
+// warp's shared-memory buffer with lane-strided 16-byte cp.async (the planner
 // starts every unit's scratch run on a 32-point boundary and pads the scratch, so
 // the copies are aligned and in bounds) and prefetches the 24 state values into L2,
 // then runs the algebra reading shared memory: the loads that kept the

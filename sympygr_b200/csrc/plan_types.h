@@ -4,7 +4,7 @@
 // into z-slabs ("units", by default at most 48 planes); a unit's points are numbered
 // compactly, x fastest:  lp = (i-3) + I0*((j-3) + I1*(k-3-k0)).  Units are packed
 // into chunks whose total point count fits the derivative scratch; each chunk is
-// evaluated by one derivative launch (one CTA per 16x16 column tile of a unit,
+// evaluated by one derivative launch (one CTA per 16x8 column tile of a unit,
 // streaming along z through all variables) followed by one algebra launch (one
 // CTA per run of consecutive points of a unit).
 #pragma once
@@ -14,10 +14,10 @@ namespace b200bssn {
 
 constexpr int kNumVars = 24;
 constexpr int kNumDerivs = 138;  // algebra inputs: 72 first + 66 second derivatives
-constexpr int kTileX = 16, kTileY = 16;
+constexpr int kTileX = 16, kTileY = 8;
 constexpr int kTileZ = 48;       // default z-slab depth (measured best on the 3000-block batch)
 constexpr int kHalo = 4;         // closure rows reach four points inward (z queue: 4 each side)
-constexpr int kDerivThreads = 256;
+constexpr int kDerivThreads = 128;
 constexpr int kAlgebraThreads = 128;
 
 struct BlockDev {

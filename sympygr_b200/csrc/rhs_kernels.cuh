@@ -1,6 +1,6 @@
 // The kernels of one right-hand-side evaluation of a chunk of blocks.
 //
-//  derivative stage     a CTA streams one variable along z through one 16x16 column
+//  derivative stage     a CTA streams one variable along z through one 16x8 column
 //                       tile of a unit and writes, per interior point, the
 //                       variable's first derivatives, its second derivatives when
 //                       it has them (mixed ones as compositions D_y(D_x u),
@@ -60,7 +60,7 @@ struct DerivArgs {
 // ---------------------------------------------------------------------------
 // Derivative kernel: a 2.5-D streaming stencil.
 //
-// A work item is one 16x16 column tile of a unit (a z-slab of up to 48 interior
+// A work item is one 16x8 column tile of a unit (a z-slab of up to 48 interior
 // planes of one block) and one variable; the CTA marches along z.  Each z step
 // brings one plane of the tile plus its 4-point x-y halo into shared memory
 // (cp.async into four plane buffers: three planes stream in while one is
@@ -75,11 +75,14 @@ struct DerivArgs {
 // rows (CL), so the items away from flagged faces carry no closure tests.
 // ---------------------------------------------------------------------------
 constexpr int kPlaneW = kTileX + 2 * kHalo;  // 24: plane width incl. halo
-constexpr int kPlaneH = kTileY + 2 * kHalo;  // 24
+constexpr int kPlaneH = kTileY + 2 * kHalo;  // 16
 constexpr int kPlane = kPlaneW * kPlaneH;     // doubles per staged plane
 constexpr int kDxRows = kTileY + 2 * kHalo;  // D_x rows kept per plane (y halo)
 constexpr int kQ = 2 * kHalo + 1;            // z queue depth (planes z-4 .. z+4)
-static_assert(kTileX == 16 && kTileY == 16 && kDerivThreads == 256, "thread tile is 16x16");
+static_assert(kTileX == 16 && kDerivThreads == kTileX * kTileY && kTileY <= 16, "one thread per tile column");
+// plane copy: each warp stages every (kDerivThreads / 32)-th row of the plane
+constexpr int kStageRows = kPlaneH / (kDerivThreads / 32);
+static_assert(kStageRows * (kDerivThreads / 32) == kPlaneH, "plane rows split evenly over the warps");
 
 __device__ __forceinline__ void cp_async8(double* smem_dst, const double* gmem_src) {
   const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
@@ -426,14 +429,15 @@ __device__ __forceinline__ void derive_tile(const DerivArgs& a, const TileDev t,
   const int zload = min(nz, zend);   // planes beyond are never loaded
   const bool clx = closure_row(gi, nx, lox, hix), cly = closure_row(gj, ny, loy, hiy);
 
-  // This thread's share of a plane copy (fixed for the whole item): column bx of
-  // the 32-wide staging grid, rows by0, by0+8, by0+16 of the 24-row plane.
+  // This thread's share of a plane copy (fixed for the whole item): column sbx of
+  // the 32-wide staging grid (24 columns used), every (warps per CTA)-th row of the
+  // plane from its warp's index on.
   const int sbx = threadIdx.x & 31, sby0 = threadIdx.x >> 5;
-  int st_soff[3], st_goff[3];
-  bool st_ok[3];
+  int st_soff[kStageRows], st_goff[kStageRows];
+  bool st_ok[kStageRows];
 #pragma unroll
-  for (int r = 0; r < 3; ++r) {
-    const int by = sby0 + 8 * r, pi = ox + sbx, pj = oy + by;
+  for (int r = 0; r < kStageRows; ++r) {
+    const int by = sby0 + (kDerivThreads / 32) * r, pi = ox + sbx, pj = oy + by;
     st_ok[r] = sbx < kPlaneW && pi >= xlo && pi < xhi && pj >= ylo && pj < yhi;
     st_soff[r] = by * kPlaneW + sbx;
     st_goff[r] = pi + nx * pj;
@@ -445,7 +449,7 @@ __device__ __forceinline__ void derive_tile(const DerivArgs& a, const TileDev t,
   bool dx_ok[2];
 #pragma unroll
   for (int r = 0; r < 2; ++r) {
-    const int yy = dyy0 + 16 * r, pj = oy + yy;
+    const int yy = dyy0 + kTileY * r, pj = oy + yy;
     dx_ok[r] = yy < kDxRows && dxx < ex && pj >= ylo && pj < yhi;
   }
   const int64_t plane_elems = (int64_t)nx * ny;
@@ -463,7 +467,7 @@ __device__ __forceinline__ void derive_tile(const DerivArgs& a, const TileDev t,
     const double* fp = f + plane_elems * zi;
     const bool in = zi < zload;
 #pragma unroll
-    for (int r = 0; r < 3; ++r) cp_async8_if(&s_plane[b][st_soff[r]], fp + st_goff[r], in && st_ok[r]);
+    for (int r = 0; r < kStageRows; ++r) cp_async8_if(&s_plane[b][st_soff[r]], fp + st_goff[r], in && st_ok[r]);
     cp_async_commit();
   };
 
@@ -479,7 +483,7 @@ __device__ __forceinline__ void derive_tile(const DerivArgs& a, const TileDev t,
 #pragma unroll
       for (int r = 0; r < 2; ++r) {
         if (dx_ok[r]) {
-          const int yy = dyy0 + 16 * r;
+          const int yy = dyy0 + kTileY * r;
           const double* p = P + yy * kPlaneW + dxx + kHalo;
           double w[7];
 #pragma unroll
@@ -607,7 +611,7 @@ __device__ __forceinline__ bool tile_has_closure(const DerivArgs& a, const TileD
 // one variable streamed through one column tile, so the launch ends with a short
 // tail whatever the mix of block sizes.
 template <typename ST>
-__global__ void __launch_bounds__(kDerivThreads, 2)
+__global__ void __launch_bounds__(kDerivThreads, 512 / kDerivThreads)
 bssn_derivs_kernel(const __grid_constant__ DerivArgs a) {
   __shared__ double s_plane[4][kPlane];
   __shared__ double s_dxp[2 * kDxRows * kTileX];
@@ -642,8 +646,11 @@ constexpr size_t kDerivSmemBytes = 0;  // all shared memory is static
 
 // The same items split by kind into two persistent kernels, one over the 11
 // variables with second derivatives and one over the 13 without: the latter needs
-// 80 registers instead of 128, so it runs 3 CTAs per SM instead of 2 (measured on
-// the batch: derivatives 70.0 -> 62.8 ms MIXED, 76.9 -> 71.0 ms FP64).  Plans launch
+// 80 registers instead of 128, so it runs 24 warps per SM instead of 16 (measured on
+// the batch, with 16x16 tiles: derivatives 70.0 -> 62.8 ms MIXED, 76.9 -> 71.0 ms FP64).
+// The CTA is a 16x8 tile of 4 warps, so each per-plane barrier waits on 4 warps
+// (16x16 tiles of 8 warps: 48.8 / 64.0 ms against 47.5 / 63.6 ms, despite the larger
+// halo share).  Plans launch
 // these; the allocation-free entry point keeps the combined kernel above.
 __device__ __forceinline__ int kind_var(bool dd, int i) {
   constexpr int kDD[11] = {0, 1, 6, 7, 8, 12, 13, 14, 15, 16, 17};  // alpha chi beta gt
@@ -651,7 +658,7 @@ __device__ __forceinline__ int kind_var(bool dd, int i) {
   return dd ? kDD[i] : kND[i];
 }
 constexpr int kKindVars[2] = {13, 11};        // [DD]
-constexpr int kKindCtasPerSm[2] = {3, 2};     // launch-bound occupancy, [DD]
+constexpr int kKindCtasPerSm[2] = {768 / kDerivThreads, 512 / kDerivThreads};     // launch-bound occupancy, [DD]
 
 template <typename ST, bool DD, bool ADV = false>
 __global__ void __launch_bounds__(kDerivThreads, kKindCtasPerSm[DD])

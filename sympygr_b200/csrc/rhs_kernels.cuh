@@ -83,6 +83,7 @@ static_assert(kTileX == 16 && kDerivThreads == kTileX * kTileY && kTileY <= 16, 
 // plane copy: each warp stages every (kDerivThreads / 32)-th row of the plane
 constexpr int kStageRows = kPlaneH / (kDerivThreads / 32);
 static_assert(kStageRows * (kDerivThreads / 32) == kPlaneH, "plane rows split evenly over the warps");
+static_assert(kDxRows <= 2 * kTileY, "two D_x halo rows per thread cover the plane");
 
 __device__ __forceinline__ void cp_async8(double* smem_dst, const double* gmem_src) {
   const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));

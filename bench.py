@@ -41,10 +41,10 @@ DERIV_FLOPS_PER_POINT = 72 * 12 + 33 * 14 + 33 * 12 + 72 * 14
 MIXED_BAR = 1e-6
 # Algorithmic bytes per interior point.  Derivative kernel: reads the 24 state
 # variables over the padded blocks (24 x 8 B x padded/interior points of the
-# batch) and writes the scratch (138 derivative slots x 8 B or 4 B, 24 KO sums x
-# 8 B).  Algebra kernel: reads the state at the point (24 x 8 B) and the scratch,
+# batch) and writes the scratch (138 derivative slots and 24 KO sums, x 8 B in FP64
+# or x 4 B in MIXED).  Algebra kernel: reads the state at the point (24 x 8 B) and the scratch,
 # writes 24 x 8 B.
-SCRATCH_BYTES = {"fp64": 138 * 8 + 24 * 8, "mixed": 138 * 4 + 24 * 8}
+SCRATCH_BYTES = {"fp64": 138 * 8 + 24 * 8, "mixed": 138 * 4 + 24 * 4}
 # DRAM bytes per interior point of each kernel measured by ncu on a large-block case
 # (profiles/ncu_derivs_algebra_large_blocks.md): derivative stage (its two kernels,
 # variables without + with second derivatives) / algebra kernel.

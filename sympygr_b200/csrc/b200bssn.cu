@@ -521,7 +521,7 @@ int b200bssn_plan_create_ex(b200bssn_ctx* ctx, const b200bssn_block* blocks, uin
     // + 512 B: the algebra kernels' copies and prefetches of a slot run are whole
     // 16-byte chunks or 32-point columns and may read past the last run's end
     e = cudaMalloc(&P->dscr[b], (size_t)nslots * P->cap * st + 512);
-    if (e == cudaSuccess) e = cudaMalloc((void**)&P->koscr[b], (size_t)kNumVars * P->cap * sizeof(double) + 512);
+    if (e == cudaSuccess) e = cudaMalloc(&P->koscr[b], (size_t)kNumVars * P->cap * st + 512);
   }
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&P->ev_fork, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaMalloc((void**)&P->d_counters, 2 * P->chunks.size() * sizeof(int));
@@ -905,7 +905,13 @@ int b200bssn_debug_block_scratch(b200bssn_ctx* ctx, double* slots, uint64_t npts
   } else {
     CK(ctx, cudaMemcpy(d.data(), P->dscr[0], nd * sizeof(double), cudaMemcpyDeviceToHost));
   }
-  CK(ctx, cudaMemcpy(ko.data(), P->koscr[0], ko.size() * sizeof(double), cudaMemcpyDeviceToHost));
+  if (P->precision == B200BSSN_MIXED) {
+    std::vector<float> tmp(ko.size());
+    CK(ctx, cudaMemcpy(tmp.data(), P->koscr[0], tmp.size() * sizeof(float), cudaMemcpyDeviceToHost));
+    for (size_t k = 0; k < ko.size(); ++k) ko[k] = tmp[k];
+  } else {
+    CK(ctx, cudaMemcpy(ko.data(), P->koscr[0], ko.size() * sizeof(double), cudaMemcpyDeviceToHost));
+  }
   auto at = [](int n, int s, uint64_t p) { return ((p >> 5) * n + s) * 32 + (p & 31); };
   for (int s = 0; s < kNumDerivs; ++s)
     for (uint64_t p = 0; p < npts; ++p) slots[s * npts + p] = d[at(ns, s, p)];

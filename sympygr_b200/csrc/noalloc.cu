@@ -193,7 +193,7 @@ extern "C" int b200bssn_rhs_noalloc(double* const* rhs_dev, const double* const*
   aa.ranges = ranges;
   da.dscr = b + kOffDeriv;
   aa.dscr = b + kOffDeriv;
-  da.koscr = reinterpret_cast<double*>(b + kOffKo);
+  da.koscr = b + kOffKo;
   aa.koscr = da.koscr;
   da.cap = aa.cap = (int32_t)kNoallocMaxPoints;
   da.tile_base = 0;

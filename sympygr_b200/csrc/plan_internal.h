@@ -63,7 +63,7 @@ struct b200bssn_plan {
   // derivative scratch: two buffers when the plan has more than one chunk, so the
   // derivative kernel of chunk c+1 can run while the algebra kernel of chunk c reads
   void* dscr[2] = {nullptr, nullptr};
-  double* koscr[2] = {nullptr, nullptr};
+  void* koscr[2] = {nullptr, nullptr};  // KO sums, stored like the slots (double or float)
   std::vector<cudaEvent_t> ev_deriv, ev_alg;  // per chunk: derivative / algebra done
   cudaEvent_t ev_fork = nullptr;
   int* d_counters = nullptr;  // per chunk: work counter of the derivative kernel

@@ -50,7 +50,7 @@ struct DerivArgs {
   const UnitDev* units;
   const TileDev* tiles;
   void* dscr;        // NS derivative slots (double or float), layout scr_index
-  double* koscr;     // kNumVars KO sums (double), layout scr_index
+  void* koscr;       // kNumVars KO sums (double or float, like dscr), layout scr_index
   int32_t cap;       // points per slot (multiple of 32); NS * cap < 2^31: 32-bit offsets
   int32_t tile_base;
   int32_t tile_count;
@@ -576,7 +576,9 @@ __device__ __forceinline__ void derive_tile(const DerivArgs& a, const TileDev t,
       const int lp = lp_col + plane_pts * (zo - k0);
       put_slot<NS, ST>(a, 3 * v + 2, lp, zrow_d1<CL, Rows>(qu, zc, cz));
       // rhs.cpp:332-369 sums (ko_x + ko_y) + ko_z
-      a.koscr[scr_index<kNumVars>(v, lp)] = __dadd_rn(kxy, zrow_ko<CL, Rows>(qu, zc, cz));
+      // summed in FP64, stored like the slots (FP32 in MIXED: the term enters the output
+      // scaled by sigma, far below the output's own scale)
+      static_cast<ST*>(a.koscr)[scr_index<kNumVars>(v, lp)] = (ST)__dadd_rn(kxy, zrow_ko<CL, Rows>(qu, zc, cz));
       if (DD) {
         const int s0 = 72 + 6 * q;
         put_slot<NS, ST>(a, s0 + 5, lp, zrow_d2<CL, Rows>(qu, zc, cz));
@@ -685,9 +687,9 @@ bssn_derivs_kind_kernel(const __grid_constant__ DerivArgs a) {
 }
 
 // Staged algebra kernel geometry: 32-point tasks (one warp each); a warp's buffer
-// holds its task's 138 slots (FP32 or FP64) and 24 KO sums (FP64) per point, laid
-// out as the blocked scratch holds them (scr_index):
-// 23,808 B (MIXED) or 41,472 B (FP64).  MIXED runs 4 warps per CTA, 2 CTAs per SM
+// holds its task's 138 slots and 24 KO sums per point (FP32 in MIXED, FP64 in FP64),
+// laid out as the blocked scratch holds them (scr_index): 20,736 B (MIXED) or
+// 41,472 B (FP64).  MIXED runs 4 warps per CTA, 2 CTAs per SM
 // (the register limit of the 255-register algebra); FP64 one warp per CTA, 5 per SM
 // (the shared-memory limit).  In the upwind mode (ADV) the buffer also holds the 72
 // advective-derivative columns: MIXED 2 warps per CTA, 3 CTAs per SM; FP64 3 per SM.
@@ -698,8 +700,7 @@ struct StageCfg {
   static constexpr int kWarps = sizeof(ST) == 4 ? (ADV ? 2 : 4) : 1;
   static constexpr int kThreads = 32 * kWarps;
   static constexpr int kMinBlocks = sizeof(ST) == 4 ? (ADV ? 3 : 2) : (ADV ? 3 : 5);
-  static constexpr size_t kBytesPerWarp =
-      (size_t)kSlots * kStageW * sizeof(ST) + (size_t)kNumVars * kStageW * sizeof(double);
+  static constexpr size_t kBytesPerWarp = (size_t)(kSlots + kNumVars) * kStageW * sizeof(ST);
   static constexpr size_t kSmemBytes = kWarps * kBytesPerWarp;
 };
 
@@ -711,7 +712,7 @@ struct AlgebraArgs {
   const UnitDev* units;
   const RangeDev* ranges;
   const void* dscr;
-  const double* koscr;
+  const void* koscr;
   int32_t cap;
   int32_t range_base;
   AlgebraParams<double> prm64;
@@ -733,17 +734,17 @@ __device__ __forceinline__ double bc_asymptotic(int v) {
 template <typename ST>
 struct GlobalScratch {
   const ST* d;       // slot 0 of the point: dscr + scr_index<kNumDerivs>(0, lp)
-  const double* ko;  // koscr + scr_index<kNumVars>(0, lp)
+  const ST* ko;      // koscr + scr_index<kNumVars>(0, lp)
   __device__ __forceinline__ ST dv(int s) const { return __ldg(d + s * 32); }
-  __device__ __forceinline__ double kov(int v) const { return __ldg(ko + v * 32); }
+  __device__ __forceinline__ double kov(int v) const { return (double)__ldg(ko + v * 32); }
 };
 
 template <typename ST>
 struct SharedScratch {
   const ST* d;       // this lane's column: d[s * kStageW]
-  const double* ko;  // ko[v * kStageW]
+  const ST* ko;      // ko[v * kStageW]
   __device__ __forceinline__ ST dv(int s) const { return d[s * kStageW]; }
-  __device__ __forceinline__ double kov(int v) const { return ko[v * kStageW]; }
+  __device__ __forceinline__ double kov(int v) const { return (double)ko[v * kStageW]; }
 };
 
 template <typename RT, class Src>
@@ -863,9 +864,9 @@ bssn_algebra_kernel(const __grid_constant__ AlgebraArgs a) {
     const int lp0 = (int)un.sbase + rg.start;
     const int b0 = lp0 >> 5, nblk = ((lp0 + rg.count - 1) >> 5) - b0 + 1;
     const char* pd = reinterpret_cast<const char*>(static_cast<const ST*>(a.dscr) + (size_t)b0 * kNumDerivs * 32);
-    const char* pk = reinterpret_cast<const char*>(a.koscr + (size_t)b0 * kNumVars * 32);
+    const char* pk = reinterpret_cast<const char*>(static_cast<const ST*>(a.koscr) + (size_t)b0 * kNumVars * 32);
     // in pieces of at most 4 KB (both runs are multiples of 16 bytes long)
-    const uint32_t td = (uint32_t)nblk * kNumDerivs * 32 * sizeof(ST), tk = (uint32_t)nblk * kNumVars * 32 * 8;
+    const uint32_t td = (uint32_t)nblk * kNumDerivs * 32 * sizeof(ST), tk = (uint32_t)nblk * kNumVars * 32 * sizeof(ST);
     const int nd = (int)((td + 4095) / 4096), nk = (int)((tk + 4095) / 4096);
     for (int k = threadIdx.x; k < nd + nk; k += kAlgebraThreads) {
       const bool dk = k < nd;
@@ -877,7 +878,7 @@ bssn_algebra_kernel(const __grid_constant__ AlgebraArgs a) {
   const int lpu = rg.start + threadIdx.x;
   const int lp = (int)un.sbase + lpu;
   const GlobalScratch<ST> src{static_cast<const ST*>(a.dscr) + scr_index<kNumDerivs>(0, lp),
-                              a.koscr + scr_index<kNumVars>(0, lp)};
+                              static_cast<const ST*>(a.koscr) + scr_index<kNumVars>(0, lp)};
   algebra_point<RT, MODE>(a, un, lpu, src);
 }
 
@@ -908,7 +909,7 @@ bssn_algebra_staged_kernel(const __grid_constant__ AlgebraArgs a, int ntasks) {
   extern __shared__ __align__(16) unsigned char s_stage[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   ST* sd = reinterpret_cast<ST*>(s_stage + warp * Cfg::kBytesPerWarp);
-  double* sk = reinterpret_cast<double*>(s_stage + warp * Cfg::kBytesPerWarp +
+  ST* sk = reinterpret_cast<ST*>(s_stage + warp * Cfg::kBytesPerWarp +
                                          Cfg::kSlots * kStageW * sizeof(ST));
   const int nwarps = gridDim.x * Cfg::kWarps;
   for (int t = blockIdx.x * Cfg::kWarps + warp; t < ntasks; t += nwarps) {
@@ -932,9 +933,9 @@ bssn_algebra_staged_kernel(const __grid_constant__ AlgebraArgs a, int ntasks) {
       // the task's slots and KO sums are one contiguous block each in the scratch
       // (scr_index; lp0 is a multiple of 32), laid out exactly as the buffer wants
       // them: copy both in 16-byte pieces, lane-strided
-      constexpr int ND = Cfg::kSlots * kStageW * (int)sizeof(ST) / 16, NK = kNumVars * kStageW * 8 / 16;
+      constexpr int ND = Cfg::kSlots * kStageW * (int)sizeof(ST) / 16, NK = kNumVars * kStageW * (int)sizeof(ST) / 16;
       const char* d = reinterpret_cast<const char*>(static_cast<const ST*>(a.dscr) + (size_t)lp0 * Cfg::kSlots);
-      const char* ko = reinterpret_cast<const char*>(a.koscr + (size_t)lp0 * kNumVars);
+      const char* ko = reinterpret_cast<const char*>(static_cast<const ST*>(a.koscr) + (size_t)lp0 * kNumVars);
 #pragma unroll 6
       for (int k = lane; k < ND; k += 32) cp_async16(reinterpret_cast<char*>(sd) + 16 * k, d + 16 * k);
 #pragma unroll 4

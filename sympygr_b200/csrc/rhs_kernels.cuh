@@ -687,20 +687,26 @@ bssn_derivs_kind_kernel(const __grid_constant__ DerivArgs a) {
 }
 
 // Staged algebra kernel geometry: 32-point tasks (one warp each); a warp's buffer
-// holds its task's 138 slots and 24 KO sums per point (FP32 in MIXED, FP64 in FP64),
-// laid out as the blocked scratch holds them (scr_index): 20,736 B (MIXED) or
-// 41,472 B (FP64).  MIXED runs 4 warps per CTA, 2 CTAs per SM
-// (the register limit of the 255-register algebra); FP64 one warp per CTA, 5 per SM
-// (the shared-memory limit).  In the upwind mode (ADV) the buffer also holds the 72
-// advective-derivative columns: MIXED 2 warps per CTA, 3 CTAs per SM; FP64 3 per SM.
+// holds its task's staged slots and 24 KO sums per point, laid out as the blocked
+// scratch holds them (scr_index).  MIXED stages all 138 slots in FP32 (20,736 B),
+// 4 warps per CTA, 2 CTAs per SM (the register limit of the 254-register algebra).
+// FP64 stages the 72 first derivatives and the KO sums (24,576 B) and reads the 66
+// second derivatives, which the Ricci stage and the outputs use, from global memory
+// after an L2 prefetch of their contiguous run: one-warp CTAs, 8 per SM (the register
+// limit; staging all 138 slots fitted only 5).  In the upwind mode (ADV) the scratch
+// also holds the 72 advective derivatives: MIXED stages them too (2 warps per CTA, 3
+// CTAs per SM), FP64 reads them from global memory like the second derivatives.
 constexpr int kStageW = 32;
 template <typename ST, bool ADV = false>
 struct StageCfg {
   static constexpr int kSlots = ADV ? kNumDerivs + 3 * kNumVars : kNumDerivs;  // 210 / 138
+  // slots copied to shared memory: all in MIXED; in FP64 the 72 first derivatives (the
+  // rest, prefetched into L2, is read from global memory), so 8 warps fit per SM
+  static constexpr int kStaged = sizeof(ST) == 4 ? kSlots : 72;
   static constexpr int kWarps = sizeof(ST) == 4 ? (ADV ? 2 : 4) : 1;
   static constexpr int kThreads = 32 * kWarps;
-  static constexpr int kMinBlocks = sizeof(ST) == 4 ? (ADV ? 3 : 2) : (ADV ? 3 : 5);
-  static constexpr size_t kBytesPerWarp = (size_t)(kSlots + kNumVars) * kStageW * sizeof(ST);
+  static constexpr int kMinBlocks = sizeof(ST) == 4 ? (ADV ? 3 : 2) : 8;
+  static constexpr size_t kBytesPerWarp = (size_t)(kStaged + kNumVars) * kStageW * sizeof(ST);
   static constexpr size_t kSmemBytes = kWarps * kBytesPerWarp;
 };
 
@@ -739,11 +745,12 @@ struct GlobalScratch {
   __device__ __forceinline__ double kov(int v) const { return (double)__ldg(ko + v * 32); }
 };
 
-template <typename ST>
+template <typename ST, int STAGED>
 struct SharedScratch {
-  const ST* d;       // this lane's column: d[s * kStageW]
+  const ST* d;       // this lane's column: d[s * kStageW], slots s < STAGED
   const ST* ko;      // ko[v * kStageW]
-  __device__ __forceinline__ ST dv(int s) const { return d[s * kStageW]; }
+  const ST* g;       // this lane's slot 0 in the scratch block (slots s >= STAGED)
+  __device__ __forceinline__ ST dv(int s) const { return s < STAGED ? d[s * kStageW] : __ldg(g + s * kStageW); }
   __device__ __forceinline__ double kov(int v) const { return (double)ko[v * kStageW]; }
 };
 
@@ -910,7 +917,7 @@ bssn_algebra_staged_kernel(const __grid_constant__ AlgebraArgs a, int ntasks) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   ST* sd = reinterpret_cast<ST*>(s_stage + warp * Cfg::kBytesPerWarp);
   ST* sk = reinterpret_cast<ST*>(s_stage + warp * Cfg::kBytesPerWarp +
-                                         Cfg::kSlots * kStageW * sizeof(ST));
+                                 Cfg::kStaged * kStageW * sizeof(ST));
   const int nwarps = gridDim.x * Cfg::kWarps;
   for (int t = blockIdx.x * Cfg::kWarps + warp; t < ntasks; t += nwarps) {
     const RangeDev rg = a.ranges[a.range_base + (t >> 2)];
@@ -933,20 +940,32 @@ bssn_algebra_staged_kernel(const __grid_constant__ AlgebraArgs a, int ntasks) {
       // the task's slots and KO sums are one contiguous block each in the scratch
       // (scr_index; lp0 is a multiple of 32), laid out exactly as the buffer wants
       // them: copy both in 16-byte pieces, lane-strided
-      constexpr int ND = Cfg::kSlots * kStageW * (int)sizeof(ST) / 16, NK = kNumVars * kStageW * (int)sizeof(ST) / 16;
+      constexpr int ND = Cfg::kStaged * kStageW * (int)sizeof(ST) / 16, NK = kNumVars * kStageW * (int)sizeof(ST) / 16;
       const char* d = reinterpret_cast<const char*>(static_cast<const ST*>(a.dscr) + (size_t)lp0 * Cfg::kSlots);
       const char* ko = reinterpret_cast<const char*>(static_cast<const ST*>(a.koscr) + (size_t)lp0 * kNumVars);
 #pragma unroll 6
       for (int k = lane; k < ND; k += 32) cp_async16(reinterpret_cast<char*>(sd) + 16 * k, d + 16 * k);
 #pragma unroll 4
       for (int k = lane; k < NK; k += 32) cp_async16(reinterpret_cast<char*>(sk) + 16 * k, ko + 16 * k);
+      if constexpr (Cfg::kStaged < Cfg::kSlots) {
+        // the unstaged slots: one contiguous run after the staged ones, into L2
+        constexpr uint32_t kRest = (Cfg::kSlots - Cfg::kStaged) * kStageW * sizeof(ST);
+        constexpr int kPieces = (int)((kRest + 4095) / 4096);
+        static_assert(kPieces <= 32, "one piece per lane");
+        if (lane < kPieces) {
+          const uint32_t off = 4096u * (uint32_t)lane;
+          prefetch_l2_bulk(d + (size_t)ND * 16 + off, min(4096u, kRest - off));
+        }
+      }
     }
     cp_async_commit();
     cp_async_wait<0>();
     __syncwarp();  // the copies of every lane are visible to the whole warp
     if (valid) {
-      const SharedScratch<ST> src{sd + lane, sk + lane};
-      algebra_point<RT, MODE, SharedScratch<ST>, ADV>(a, un, lpu, src);
+      using Src = SharedScratch<ST, Cfg::kStaged>;
+      const Src src{sd + lane, sk + lane,
+                    static_cast<const ST*>(a.dscr) + (size_t)lp0 * Cfg::kSlots + lane};
+      algebra_point<RT, MODE, Src, ADV>(a, un, lpu, src);
     }
   }
 }

@@ -31,6 +31,9 @@ sys.path.insert(0, REPO)
 METRIC = "BSSN RHS Mpoints/s, mixed vs plain FP64 on 1 B200 at <=1e-6 rel err; %roofline"
 UNIT = "Mpoints/s"
 SIGMA = 0.4
+# the workload both arms report (the precision of each is in its `dtype`)
+WORKLOAD = ("two-puncture Brill-Lindquist batch: 3000 blocks, padded 13/21/37/69/135 "
+            "(1800/750/300/120/30), KO sigma 0.4")
 # Algorithmic work per interior point.  Algebra: the operation count of the staged,
 # generated device function (sympy count_ops, an FMA counted as 2) plus the KO add
 # (2 per variable) and the eta damping (~10).  Derivatives: 72 first derivatives
@@ -257,8 +260,8 @@ def reference_arm(args, rank, world):
         "n_gpus": world, "steps": len(times), "warmup": min(args.warmup, 1),
         "ms_per_step": round(t * 1e3, 2), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "two-puncture Brill-Lindquist batch, 3000 blocks 13^3..135^3",
-                   "sample": sample_desc},
+        "config": {"workload": WORKLOAD, "blocks": len(blocks),
+                   "interior_points_per_gpu": sum(b.ninterior for b in blocks), "sample": sample_desc},
         "cpu_baseline": {"value": round(val, 4), "unit": UNIT, "cores": ncores, "kind": "reference",
                          "sample": sample_desc},
         "e2e": {"value": round(val, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -497,9 +500,7 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_mixed, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64 state+stencils / f32 algebra", "data": "synthetic",
-            "config": {"workload": "two-puncture Brill-Lindquist batch: 3000 blocks, padded 13/21/37/69/135 "
-                                   "(1800/750/300/120/30), KO sigma 0.4, mixed precision",
-                       "blocks": len(blocks), "interior_points_per_gpu": npts,
+            "config": {"workload": WORKLOAD, "blocks": len(blocks), "interior_points_per_gpu": npts,
                        "l2": "inputs (26.7 GB per state) larger than L2; no flush",
                        "scale": args.scale},
             "fp64": {"value": round(val_fp64, 3), "ms_per_step": round(ms_fp64, 3),

@@ -85,10 +85,6 @@ constexpr int kStageRows = kPlaneH / (kDerivThreads / 32);
 static_assert(kStageRows * (kDerivThreads / 32) == kPlaneH, "plane rows split evenly over the warps");
 static_assert(kDxRows <= 2 * kTileY, "two D_x halo rows per thread cover the plane");
 
-__device__ __forceinline__ void cp_async8(double* smem_dst, const double* gmem_src) {
-  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem_src) : "memory");
-}
 // the copy is issued only when `p` holds; otherwise nothing is read or written
 __device__ __forceinline__ void cp_async8_if(double* smem_dst, const double* gmem_src, bool p) {
   const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));

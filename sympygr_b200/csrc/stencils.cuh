@@ -309,21 +309,6 @@ __device__ __forceinline__ double win_ko(const double (&w)[N], const int C,
   return __dmul_rn(c.ko_c, a);
 }
 
-// Out-of-line closure evaluations: only points next to flagged faces take them,
-// so keeping them out of the unrolled window loops keeps those loops small.
-static __device__ __noinline__ double line_d1_cl(const double* p, int s, int pos, int n, bool lo, bool hi,
-                                          const LineScales& c) {
-  return line_d1(p, s, pos, n, lo, hi, c);
-}
-static __device__ __noinline__ double line_d2_cl(const double* p, int s, int pos, int n, bool lo, bool hi,
-                                          const LineScales& c) {
-  return line_d2(p, s, pos, n, lo, hi, c);
-}
-static __device__ __noinline__ double line_ko_cl(const double* p, int s, int pos, int n, bool lo, bool hi,
-                                          const LineScales& c) {
-  return line_ko(p, s, pos, n, lo, hi, c);
-}
-
 // True when the point at padded index `pos` takes a closure row.
 __device__ __forceinline__ bool closure_row(int pos, int n, bool lo, bool hi) {
   return (lo && pos < 6) || (hi && pos >= n - 6);

@@ -930,6 +930,14 @@ bssn_algebra_staged_kernel(const __grid_constant__ AlgebraArgs a, int ntasks) {
       const int64_t pp = B.offset + (lx + 3) + (int64_t)B.sz[0] * ((ly + 3) + (int64_t)B.sz[1] * (lz + 3 + un.k0));
 #pragma unroll
       for (int v = 0; v < kNumVars; ++v) prefetch_l2(a.u[v] + pp);
+      if constexpr (MODE == RK_MIDDLE || MODE == RK_LAST) {
+        // the stage update reads u^n and the accumulator at every output
+#pragma unroll
+        for (int v = 0; v < kNumVars; ++v) {
+          prefetch_l2(a.rk.base[v] + pp);
+          prefetch_l2(a.rk.acc[v] + pp);
+        }
+      }
     }
     __syncwarp();  // every lane is done reading the previous task's buffer
     {

@@ -51,7 +51,7 @@ SCRATCH_BYTES = {"fp64": 138 * 8 + 24 * 8, "mixed": 138 * 4 + 24 * 4}
 # DRAM bytes per interior point of each kernel measured by ncu on a large-block case
 # (profiles/ncu_derivs_algebra_large_blocks.md): derivative stage (its two kernels,
 # variables without + with second derivatives) / algebra kernel.
-NCU_TRAFFIC_PER_POINT = {"mixed": (402.0 + 659.0, 1125.0), "fp64": (596.0 + 1127.0, 2108.0)}
+NCU_TRAFFIC_PER_POINT = {"mixed": (376.0 + 646.0, 1123.0), "fp64": (584.0 + 1122.0, 2110.0)}
 
 PG_TIMEOUT_S = 120  # process-group timeout under torchrun (N > 1)
 

@@ -645,11 +645,12 @@ constexpr size_t kDerivSmemBytes = 0;  // all shared memory is static
 
 // The same items split by kind into two persistent kernels, one over the 11
 // variables with second derivatives and one over the 13 without: the latter needs
-// 80 registers instead of 128, so it runs 24 warps per SM instead of 16 (measured on
-// the batch, with 16x16 tiles: derivatives 70.0 -> 62.8 ms MIXED, 76.9 -> 71.0 ms FP64).
-// The CTA is a 16x8 tile of 4 warps, so each per-plane barrier waits on 4 warps
-// (16x16 tiles of 8 warps: 48.8 / 64.0 ms against 47.5 / 63.6 ms, despite the larger
-// halo share).  Plans launch
+// fewer registers than 128, so it runs more warps per SM (measured on the batch, with
+// 16x16 tiles, 80 registers against 128: derivatives 70.0 -> 62.8 ms MIXED, 76.9 ->
+// 71.0 ms FP64); it now runs 5 CTAs per SM at up to 96 registers without spills (6 at
+// 80: MIXED the same, FP64 1 % slower).  The CTA is a 16x8 tile of 4 warps, so each
+// per-plane barrier waits on 4 warps (16x16 tiles of 8 warps: 48.8 / 64.0 ms against
+// 47.5 / 63.6 ms, despite the larger halo share).  Plans launch
 // these; the allocation-free entry point keeps the combined kernel above.
 __device__ __forceinline__ int kind_var(bool dd, int i) {
   constexpr int kDD[11] = {0, 1, 6, 7, 8, 12, 13, 14, 15, 16, 17};  // alpha chi beta gt
@@ -657,10 +658,14 @@ __device__ __forceinline__ int kind_var(bool dd, int i) {
   return dd ? kDD[i] : kND[i];
 }
 constexpr int kKindVars[2] = {13, 11};        // [DD]
-constexpr int kKindCtasPerSm[2] = {768 / kDerivThreads, 512 / kDerivThreads};     // launch-bound occupancy, [DD]
+// launch-bound occupancy of a kind kernel: the upwind first-derivative kind keeps 6
+// CTAs per SM (80 registers; 5 measured 4 % slower there)
+constexpr int kind_ctas_per_sm(bool dd, bool adv) {
+  return (dd ? 512 : (adv ? 768 : 640)) / kDerivThreads;
+}
 
 template <typename ST, bool DD, bool ADV = false>
-__global__ void __launch_bounds__(kDerivThreads, kKindCtasPerSm[DD])
+__global__ void __launch_bounds__(kDerivThreads, kind_ctas_per_sm(DD, ADV))
 bssn_derivs_kind_kernel(const __grid_constant__ DerivArgs a) {
   constexpr int NV = kKindVars[DD];
   __shared__ double s_plane[4][kPlane];

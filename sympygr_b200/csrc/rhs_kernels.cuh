@@ -439,7 +439,7 @@ __device__ __forceinline__ void derive_tile(const DerivArgs& a, const TileDev t,
     st_soff[r] = by * kPlaneW + sbx;
     st_goff[r] = pi + nx * pj;
   }
-  // and of the y-halo D_x rows: column dxx, rows dyy0 and dyy0 + 16
+  // and of the y-halo D_x rows: column dxx, rows dyy0 and dyy0 + kTileY
   const int dxx = threadIdx.x & 15, dyy0 = threadIdx.x >> 4;
   const int dpi = i0 + dxx;
   const bool dcl = closure_row(dpi, nx, lox, hix);

@@ -10,6 +10,7 @@ no flush is needed between steps).  `value` is the MIXED-precision throughput
 path is timed the same way and reported beside it.
 
     python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+    python bench.py --profile-case {mixed,fp64} [--profile-steps N]   # small ncu case
 
 Multi-GPU (torchrun): every rank evaluates its own batch (weak scaling, no
 collective on the data path); time = max over ranks.
@@ -34,24 +35,28 @@ SIGMA = 0.4
 # the workload both arms report (the precision of each is in its `dtype`)
 WORKLOAD = ("two-puncture Brill-Lindquist batch: 3000 blocks, padded 13/21/37/69/135 "
             "(1800/750/300/120/30), KO sigma 0.4")
-# Algorithmic work per interior point.  Algebra: the operation count of the staged,
-# generated device function (sympy count_ops, an FMA counted as 2) plus the KO add
-# (2 per variable) and the eta damping (~10).  Derivatives: 72 first derivatives
-# x 12 flops (6-point stencil, multiply-add each), 33 second derivatives x 14,
-# 33 mixed (a first derivative of a first derivative) x 12, KO 72 x 14.
-ALGEBRA_FLOPS_PER_POINT = 2428 + 48 + 10
-DERIV_FLOPS_PER_POINT = 72 * 12 + 33 * 14 + 33 * 12 + 72 * 14
 MIXED_BAR = 1e-6
-# Algorithmic bytes per interior point.  Derivative kernel: reads the 24 state
-# variables over the padded blocks (24 x 8 B x padded/interior points of the
-# batch) and writes the scratch (138 derivative slots and 24 KO sums, x 8 B in FP64
-# or x 4 B in MIXED).  Algebra kernel: reads the state at the point (24 x 8 B) and the scratch,
-# writes 24 x 8 B.
-SCRATCH_BYTES = {"fp64": 138 * 8 + 24 * 8, "mixed": 138 * 4 + 24 * 4}
-# DRAM bytes per interior point of each kernel measured by ncu on a large-block case
-# (profiles/ncu_derivs_algebra_large_blocks.md): derivative stage (its two kernels,
-# variables without + with second derivatives) / algebra kernel.
-NCU_TRAFFIC_PER_POINT = {"mixed": (376.0 + 646.0, 1123.0), "fp64": (584.0 + 1122.0, 2110.0)}
+
+# Algorithmic work per interior point of the reference's algorithm (bssnrhs,
+# bssn/src/rhs.cpp:80-388):
+#  * the per-point algebra: 4137 operations after the reference's CSE
+#    (bssn/src/bssneqs_eta_const_standard_gauge.cpp:1028);
+#  * the stencils: 105 first derivatives (72 + 33 mixed) x 12, 33 diagonal second
+#    derivatives x 14, 72 KO rows x 14, the KO add 24 x 4, eta damping ~10.
+# FP64 path: all of it in FP64.  MIXED: the algebra in FP32, the stencils in FP64
+# (their differences; the weighted sums of the split-precision rows run in FP32).
+FLOPS_ALGEBRA = 4137
+FLOPS_STENCIL = 105 * 12 + 33 * 14 + 72 * 14 + 24 * 4 + 10
+# Bytes per interior point an evaluation must move at the least: the 24 state
+# variables over the padded blocks (read) and the 24 right-hand sides (written).
+BYTES_VARS = 24 * 8
+# DRAM bytes per interior point of each kernel of an evaluation, from an ncu capture
+# (dram__bytes_read.sum + dram__bytes_write.sum) of a 3.15M-point case of the batch's
+# large blocks (four 69^3 and one 135^3, one flagged face): `python bench.py
+# --profile-case {mixed,fp64}`.
+NCU_TRAFFIC_PER_POINT = {"mixed": {"derivs": 376.0 + 646.0, "algebra": 1123.0, "single_pass": None},
+                         "fp64": {"derivs": 584.0 + 1122.0, "algebra": 2110.0}}
+REF_STEP_CAP, REF_WARMUP_CAP = 3, 1  # reference arm: ~32 s per full-batch step on 16 threads
 
 PG_TIMEOUT_S = 120  # process-group timeout under torchrun (N > 1)
 
@@ -179,6 +184,39 @@ class ClockSampler:
                 "power_w_max": max(power) if power else None}
 
 
+def host_cpu() -> dict:
+    """This host's CPU: model, logical CPUs, physical cores (distinct (package, core)
+    pairs of /proc/cpuinfo; sockets x cores per socket from lscpu where that is absent)."""
+    model, pairs, phys, core = None, set(), None, None
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                k, _, v = line.partition(":")
+                k, v = k.strip(), v.strip()
+                if k == "model name" and model is None:
+                    model = v
+                elif k == "physical id":
+                    phys = v
+                elif k == "core id":
+                    core = v
+                elif k == "" and phys is not None and core is not None:
+                    pairs.add((phys, core))
+                    phys = core = None
+        if phys is not None and core is not None:
+            pairs.add((phys, core))
+    except OSError:
+        pass
+    physical = len(pairs) or None
+    if physical is None:
+        try:
+            out = subprocess.run(["lscpu"], capture_output=True, text=True, timeout=10).stdout
+            kv = dict(ln.split(":", 1) for ln in out.splitlines() if ":" in ln)
+            physical = int(kv["Socket(s)"].strip()) * int(kv["Core(s) per socket"].strip())
+        except Exception:
+            physical = None
+    return {"model": model, "logical": os.cpu_count() or 1, "physical_cores": physical}
+
+
 def stratified_blocks(blocks, frac):
     """A class-proportional subset of a block list (at least one block per class)."""
     by = {}
@@ -191,21 +229,15 @@ def stratified_blocks(blocks, frac):
     return out
 
 
-def cpu_reference_run(u_host, blocks, nthreads):
-    """The reference's own CPU bssnrhs (compiled from its sources, -O3) over a block
-    list in its block-parallel OpenMP loop; returns (seconds, interior points)."""
-    import numpy as np
-
-    from oracle import pyoracle as po
-
-    rhs = np.zeros_like(u_host)
-    prm = po.params(ko_sigma=SIGMA)
-    secs = po.ref_blocks_omp(u_host, rhs, blocks, prm, nthreads=nthreads, flavour="fast")
-    return secs, sum(b.ninterior for b in blocks)
+def workload_config(nblocks: int, npts: int) -> dict:
+    """The `config` object of both arms (identical, so the two lines compare)."""
+    return {"workload": WORKLOAD, "blocks": nblocks, "interior_points_per_gpu": npts,
+            "l2": "inputs (26.7 GB per state) larger than L2; no flush"}
 
 
-def compact_host_batch(blocks):
-    """Host arrays for a block subset, re-offset compactly (numpy generator)."""
+def compact(u_src, blocks, device_to_host=True):
+    """The given blocks' slices of a [24, N] array (numpy or torch), re-offset compactly
+    into a host numpy array (block starts 32-element aligned); returns (u, blocks)."""
     import numpy as np
 
     from sympygr_b200 import workloads as wl
@@ -213,13 +245,297 @@ def compact_host_batch(blocks):
     out, off = [], 0
     for b in blocks:
         out.append(wl.Block(off, b.sz, b.bflag, b.pmin, b.pmax))
-        off += b.npad
+        off += ((b.npad + 31) // 32) * 32
+    u = np.zeros((24, off))
+    for b, o in zip(blocks, out):
+        seg = u_src[:, b.offset:b.offset + b.npad]
+        u[:, o.offset:o.offset + o.npad] = seg.cpu().numpy() if hasattr(seg, "cpu") else seg
+    return u, out
+
+
+def host_batch(blocks):
+    """Host arrays for a block subset of the batch, re-offset compactly (block starts
+    32-element aligned), filled with the two-puncture fields by numpy."""
+    import numpy as np
+
+    from sympygr_b200 import workloads as wl
+
+    out, off = [], 0
+    for b in blocks:
+        out.append(wl.Block(off, b.sz, b.bflag, b.pmin, b.pmax))
+        off += ((b.npad + 31) // 32) * 32
     u = np.zeros((24, off))
     punct = [(-4.0, 0.0, 0.0, 0.5), (4.0, 0.0, 0.0, 0.5)]
     for b in out:
         x, y, z = wl.coords(b)
         wl._bl_fields(u, slice(b.offset, b.offset + b.npad), x, y, z, punct)
     return u, out
+
+
+def cpu_reference_run(u_host, blocks, nthreads, flavour="fast"):
+    """The reference's own CPU bssnrhs (compiled from its sources) over a block list
+    in its block-parallel OpenMP loop; returns (seconds, interior points, rhs)."""
+    import numpy as np
+
+    from oracle import pyoracle as po
+
+    rhs = np.zeros_like(u_host)
+    prm = po.params(ko_sigma=SIGMA)
+    secs = po.ref_blocks_omp(u_host, rhs, blocks, prm, nthreads=nthreads, flavour=flavour)
+    return secs, sum(b.ninterior for b in blocks), rhs
+
+
+def reference_arm(args, rank, world):
+    """`--impl reference`: the reference's CPU bssnrhs on this host's cores over the
+    whole 3000-block batch (or the `--ref-fraction` class-proportional sample)."""
+    if rank != 0:
+        return None
+    from oracle import pyoracle as po
+    from sympygr_b200 import workloads as wl
+
+    if not po.have_reference("fast"):
+        return {"impl": "reference", "unavailable": "reference build oracle/_ref/libbssn_ref_fast*.so missing"}
+    cpu = host_cpu()
+    nthreads = cpu["logical"]
+    frac = args.ref_fraction if 0 < args.ref_fraction < 1 else 1.0
+    blocks, _ = wl.batch_blocks(seed=0)
+    npts_all = sum(b.ninterior for b in blocks)
+    sample = blocks if frac >= 1.0 else stratified_blocks(blocks, frac)
+    # the batch's data on the host (the GPU arm's fields, computed with numpy)
+    u, sblocks = host_batch(sample)
+    # big blocks first so the block-parallel loop does not end on a long tail
+    sblocks = sorted(sblocks, key=lambda b: -b.npad)
+    warm = max(0, min(args.warmup, REF_WARMUP_CAP))
+    steps = max(1, min(args.steps, REF_STEP_CAP))
+    for _ in range(warm):
+        cpu_reference_run(u, sblocks, nthreads)
+    times, pts = [], 0
+    for _ in range(steps):
+        s, pts, _ = cpu_reference_run(u, sblocks, nthreads)
+        times.append(s)
+    t = statistics.median(times)
+    val = pts / t / 1e6
+    flav = os.path.basename(po.fast_flavour_path())
+    sample_desc = ((f"the whole batch ({pts} interior points)" if frac >= 1.0 else
+                    f"{len(sblocks)} of 3000 blocks ({frac:.3g} class-proportional sample, {pts} interior points)")
+                   + f", largest blocks first, {nthreads} OpenMP threads over blocks; {flav}; "
+                     f"median of {len(times)} steps after {warm} warm-up (capped at {REF_STEP_CAP} "
+                     f"and {REF_WARMUP_CAP}: about 30 s per step)")
+    return {
+        "metric": METRIC, "value": round(val, 4), "unit": UNIT, "impl": "reference",
+        "n_gpus": world, "steps": len(times), "warmup": warm,
+        "ms_per_step": round(t * 1e3, 2), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": workload_config(len(blocks), npts_all),
+        "steps_cap": {"steps": REF_STEP_CAP, "warmup": REF_WARMUP_CAP,
+                      "requested": {"steps": args.steps, "warmup": args.warmup}},
+        "cpu_baseline": {"value": round(val, 4), "unit": UNIT, "cores": nthreads, "kind": "reference",
+                         "physical_cores": cpu["physical_cores"], "cpu_model": cpu["model"],
+                         "build": flav, "sample": sample_desc},
+        "e2e": {"value": round(val, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def roofline(kernel, ms, npts, bytes_pp, f64_pp, f32_pp, hbm_peak, peak64, peak32, traffic_pp=None,
+             launches=1, peak_src=""):
+    """Roofline of one kernel (or a whole evaluation) from algorithmic work per point:
+    `achieved`/`peak` against HBM (the contract's object), the FP64/FP32 pipe time
+    beside it, and which roof binds (the longer of the two lower bounds)."""
+    secs = ms * 1e-3
+    gbs = bytes_pp * npts / secs / 1e9
+    t_hbm = bytes_pp * npts / (hbm_peak * 1e9)
+    # FP64 and FP32 arithmetic run on different pipes: the pipe bound is the longer one
+    t_pipe = max(f64_pp * npts / (peak64 * 1e12), f32_pp * npts / (peak32 * 1e12))
+    out = {"kernel": kernel, "bound": "hbm", "achieved": round(gbs, 1), "peak": hbm_peak, "unit": "GB/s",
+           "frac": round(gbs / hbm_peak, 4),
+           "traffic": None if traffic_pp is None else round(traffic_pp * npts / launches),
+           "bytes_per_point": round(bytes_pp, 1), "launches_per_step": launches,
+           "peak_source": peak_src,
+           "pipe": {"fp64_flops_per_point": f64_pp, "fp32_flops_per_point": f32_pp,
+                    "fp64_tflops": round(f64_pp * npts / secs / 1e12, 3),
+                    "fp32_tflops": round(f32_pp * npts / secs / 1e12, 3),
+                    "fp64_peak": round(peak64, 2), "fp32_peak": round(peak32, 2),
+                    "frac": round(t_pipe / secs, 4),
+                    "peak_source": "measured FMA-chain microbenchmark (b200bssn_fma_peak), this GPU"},
+           "binding": "hbm" if t_hbm >= t_pipe else ("fp64 pipe" if f64_pp / peak64 >= f32_pp / peak32 else "fp32 pipe"),
+           "frac_binding": round(max(t_hbm, t_pipe) / secs, 4)}
+    if traffic_pp is not None:
+        out["traffic_per_point"] = round(traffic_pp, 1)
+        out["traffic_over_algorithmic"] = round(traffic_pp / bytes_pp, 2)
+    return out
+
+
+def profile_case(args):
+    """Small case for ncu captures: four 69^3 blocks and one 135^3 block of the
+    two-puncture batch, one with a flagged face (3.15M interior points, ~0.6 GB per
+    state, larger than L2), evaluated twice with one plan; with --profile-steps also
+    the constraint kernel once and that many RK4 steps."""
+    import torch
+
+    import sympygr_b200 as sg
+    from sympygr_b200 import workloads as wl
+
+    prec = sg.FP64 if args.profile_case == "fp64" else sg.MIXED
+    # seed 5: one of the 69^3 blocks has a flagged face (8 % of the points), like the
+    # 3000-block batch (about 10 % of its points lie in blocks with flagged faces)
+    u, blocks = wl.two_puncture_batch_torch((69, 135), (4, 1), seed=5, device="cuda")
+    rhs = torch.zeros_like(u)
+    ctx = sg.Context(0)
+    plan = sg.Plan(ctx, blocks, prec)
+    prm = sg.Params.make(ko_sigma=SIGMA, precision=prec)
+    for _ in range(2):
+        plan.rhs_device(list(rhs), list(u), prm)
+    if args.profile_steps:
+        norms = torch.zeros(len(blocks) * 8, dtype=torch.float64, device="cuda")
+        plan.constraints_device(list(u), None, norms)
+        rk = sg.RK4(plan)
+        rk.init(list(u))
+        for _ in range(args.profile_steps):
+            rk.step(list(u), 1e-3, prm)
+        torch.cuda.synchronize()
+        rk.close()
+    torch.cuda.synchronize()
+    print(json.dumps({"profile_case": args.profile_case, "points": plan.points, "launches": plan.launches}))
+    plan.close()
+    ctx.close()
+
+
+def single_block_rates(ctx, reps=5):
+    """Mpoints/s of the two single-block configurations -- a 38^3 block of seeded
+    sines on flat space and a 134^3 Brill-Lindquist block with all faces flagged --
+    through the drop-in b200bssn_rhs (host arrays: copy in, evaluate, copy the
+    interior out; the path the bssnrhs shim takes) and through a plan on device arrays,
+    FP64 and MIXED.  Returns (rates, host inputs) -- the inputs feed the CPU baseline."""
+    import numpy as np
+    import torch
+
+    import sympygr_b200 as sg
+    from sympygr_b200 import workloads as wl
+
+    out, inputs = {}, {}
+    for name, (u, blk) in (("cfg1_38_sines", wl.flat_sines(38, 0.1, 0)),
+                           ("cfg2_134_brill_lindquist", wl.brill_lindquist(134, 8.0, 1.0))):
+        inputs[name] = (u, blk)
+        rhs = np.zeros_like(u)
+        ud = torch.from_numpy(u).cuda()
+        rd = torch.zeros_like(ud)
+        rec = {"interior_points": blk.ninterior}
+        for prec, pname in ((sg.FP64, "fp64"), (sg.MIXED, "mixed")):
+            prm = sg.Params.make(ko_sigma=SIGMA, precision=prec)
+            # drop-in on host arrays (synchronous): wall clock around the calls
+            sg.bssnrhs(ctx, list(rhs), list(u), blk.offset, blk.pmin, blk.pmax, blk.sz, blk.bflag, prm)
+            t0 = time.perf_counter()
+            for _ in range(reps):
+                sg.bssnrhs(ctx, list(rhs), list(u), blk.offset, blk.pmin, blk.pmax, blk.sz, blk.bflag, prm)
+            t_host = (time.perf_counter() - t0) / reps
+            plan = sg.Plan(ctx, [blk], prec)
+            stream = torch.cuda.ExternalStream(ctx.stream)
+            for _ in range(3):
+                plan.rhs_device(list(rd), list(ud), prm)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(reps):
+                plan.rhs_device(list(rd), list(ud), prm)
+            e1.record(stream)
+            e1.synchronize()
+            t_dev = e0.elapsed_time(e1) * 1e-3 / reps
+            plan.close()
+            rec[pname] = {"dropin_host_mpts": round(blk.ninterior / t_host / 1e6, 2),
+                          "dropin_host_ms": round(t_host * 1e3, 3),
+                          "plan_device_mpts": round(blk.ninterior / t_dev / 1e6, 2),
+                          "plan_device_ms": round(t_dev * 1e3, 3)}
+        out[name] = rec
+        del ud, rd
+    return out, inputs
+
+
+def cpu_baseline_leg(u_dev, blocks, rhs64_dev, single_inputs, ref_frac):
+    """The reference's own CPU bssnrhs (timing build) on this host's cores: over a
+    bounded class-proportional sample of the batch (the inputs copied from the GPU
+    arm's device arrays) and on the two single-block configurations.  Also the FP64
+    GPU path against the reference's parity build (-ffp-contract=off) on one block of
+    each size class of that sample (flagged faces where the class has them)."""
+    import numpy as np
+
+    from oracle import pyoracle as po
+
+    if not po.have_reference("fast"):
+        return None, None
+    cpu = host_cpu()
+    nthreads = cpu["logical"]
+    sample = stratified_blocks(blocks, ref_frac)
+    uh, sb = compact(u_dev, sample)
+    order = sorted(range(len(sb)), key=lambda i: -sb[i].npad)
+    secs, pts, _ = cpu_reference_run(uh, [sb[i] for i in order], nthreads)
+    flav = os.path.basename(po.fast_flavour_path())
+    per_config = {"cfg3_batch_sample": {"mpts": round(pts / secs / 1e6, 4), "seconds": round(secs, 2),
+                                        "interior_points": pts, "threads": nthreads}}
+    for name, (u, blk) in single_inputs.items():
+        # the reference parallelises over blocks only: one block runs on one thread
+        s, p, _ = cpu_reference_run(u, [blk], nthreads)
+        per_config[name] = {"mpts": round(p / s / 1e6, 4), "seconds": round(s, 2), "interior_points": p,
+                            "threads": 1}
+    cpu_rec = {"value": per_config["cfg3_batch_sample"]["mpts"], "unit": UNIT, "cores": nthreads,
+               "kind": "reference", "physical_cores": cpu["physical_cores"], "cpu_model": cpu["model"],
+               "build": flav,
+               "sample": f"{len(sb)} blocks ({ref_frac:.3g} class-proportional sample of the batch, "
+                         f"{pts} interior points, largest first), one pass, {secs:.2f} s, "
+                         f"{nthreads} OpenMP threads over blocks",
+               "per_config": per_config}
+    # FP64 GPU vs the reference (parity build) on one block per class of the sample
+    chk = []
+    for n in sorted({b.sz[0] for b in blocks}):
+        cls = [b for b in blocks if b.sz[0] == n]
+        flagged = [b for b in cls if b.bflag]
+        chk.append(flagged[0] if flagged else cls[0])
+    uc, cb = compact(u_dev, chk)
+    _, _, ref = cpu_reference_run(uc, cb, nthreads, flavour="parity")
+    got, _ = compact(rhs64_dev, chk)
+    worst, per_block = 0.0, []
+    for b in cb:
+        mx, _ = po.rel_errors(po.interior(got, b), po.interior(ref, b))
+        nz = np.abs(po.interior(ref, b)).max(axis=1) > 0
+        e = float(mx[nz].max()) if nz.any() else 0.0
+        worst = max(worst, e)
+        per_block.append({"n": b.sz[0], "bflag": b.bflag, "max_rel_err": float(f"{e:.3g}")})
+    fp64_check = {"max_rel_err": worst, "bar": 1e-12, "blocks": per_block,
+                  "against": "the reference's bssnrhs, parity build (-O2 -ffp-contract=off)"}
+    return cpu_rec, fp64_check
+
+
+def e2e_leg(ctx, blocks, u, args, dist, world):
+    """The metric end to end through the host API (b200bssn_rhs_plan_host: H2D of the
+    state, evaluate, D2H of the RHS, pinned host arrays), MIXED and FP64.  Each rank pins
+    a state and an RHS copy of its batch; where the ranks on this node would need more
+    than 60 % of its available memory, each times a class-proportional sample."""
+    import torch
+
+    import sympygr_b200 as sg
+    from sympygr_b200 import workloads as wl
+
+    local = max(1, _env_int("LOCAL_WORLD_SIZE", world))
+    span = max(b.offset + b.npad for b in blocks)
+    need = 2 * 24 * span * 8
+    budget = int(0.6 * host_bytes_available() / local)
+    hblocks, sample_note = blocks, None
+    if need > budget:
+        sub = stratified_blocks(blocks, 0.9 * budget / need)
+        hblocks, off = [], 0
+        for b in sub:
+            hblocks.append(wl.Block(off, b.sz, b.bflag, b.pmin, b.pmax))
+            off += b.npad
+        u_h = torch.empty((24, off), dtype=u.dtype, pin_memory=True)
+        for b, hb in zip(sub, hblocks):
+            u_h[:, hb.offset:hb.offset + hb.npad].copy_(u[:, b.offset:b.offset + b.npad])
+        span = off
+        sample_note = (f"{len(hblocks)} of {len(blocks)} blocks per rank (class-proportional): "
+                       f"the full batch's host buffers ({need / 1e9:.1f} GB per rank) exceed "
+                       f"60 % of this node's available memory over {local} ranks")
+    else:
+        u_h = torch.empty(tuple(u.shape), dtype=u.dtype, pin_memory=True)
+        u_h.copy_(u)
+    return u_h, hblocks, span, sample_note
 
 
 def host_bytes_available() -> int:
@@ -234,52 +550,6 @@ def host_bytes_available() -> int:
     return os.sysconf("SC_PAGE_SIZE") * os.sysconf("SC_PHYS_PAGES")
 
 
-def ref_fraction(args):
-    if args.ref_fraction > 0:
-        return min(1.0, args.ref_fraction)
-    return max(0.1, min(1.0, (os.cpu_count() or 1) / 30.0))
-
-
-def reference_arm(args, rank, world):
-    """`--impl reference`: the reference's CPU bssnrhs on this host's cores."""
-    if rank != 0:
-        return None
-    from oracle import pyoracle as po
-    from sympygr_b200 import workloads as wl
-
-    if not po.have_reference("fast"):
-        return {"impl": "reference", "unavailable": "reference build oracle/_ref/libbssn_ref_fast.so missing"}
-    ncores = os.cpu_count() or 1
-    blocks, _ = wl.batch_blocks(seed=0)
-    frac = ref_fraction(args)
-    sample = stratified_blocks(blocks, frac)
-    u, sblocks = compact_host_batch(sample)
-    # big blocks first so the block-parallel loop does not end on a long tail
-    order = sorted(range(len(sblocks)), key=lambda i: -sblocks[i].npad)
-    sblocks = [sblocks[i] for i in order]
-    for _ in range(max(0, min(args.warmup, 1))):
-        cpu_reference_run(u, sblocks, ncores)
-    times, pts = [], 0
-    for _ in range(max(1, min(args.steps, 3))):
-        s, pts = cpu_reference_run(u, sblocks, ncores)
-        times.append(s)
-    t = statistics.median(times)
-    val = pts / t / 1e6
-    sample_desc = (f"{len(sblocks)} of 3000 blocks ({frac:.3g} class-proportional sample, "
-                   f"{pts} interior points, largest blocks first) per step; median of {len(times)} steps")
-    return {
-        "metric": METRIC, "value": round(val, 4), "unit": UNIT, "impl": "reference",
-        "n_gpus": world, "steps": len(times), "warmup": min(args.warmup, 1),
-        "ms_per_step": round(t * 1e3, 2), "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "blocks": len(blocks),
-                   "interior_points_per_gpu": sum(b.ninterior for b in blocks), "sample": sample_desc},
-        "cpu_baseline": {"value": round(val, 4), "unit": UNIT, "cores": ncores, "kind": "reference",
-                         "sample": sample_desc},
-        "e2e": {"value": round(val, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-    }
-
-
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -292,12 +562,21 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-upwind", action="store_true", help="skip timing the opt-in upwind mode")
+    ap.add_argument("--no-single", action="store_true", help="skip the single-block configurations")
     ap.add_argument("--ref-fraction", type=float, default=0.0,
-                    help="class-proportional block sample for the CPU reference; 0 = enough "
-                         "135^3 blocks to give every host core one (min 0.1)")
+                    help="reference arm: class-proportional sample of the batch (0 or >= 1: the whole "
+                         "batch); GPU arm's CPU-baseline leg: its sample (0: enough 135^3 blocks to "
+                         "give every host core one, min 0.1)")
     ap.add_argument("--chunk-points", type=int, default=0)
     ap.add_argument("--slab-depth", type=int, default=0)
     ap.add_argument("--deriv-ctas", type=int, default=0, help="derivative CTAs per SM (0: max)")
+    ap.add_argument("--single-pass", action="store_true",
+                    help="MIXED headline on the one-pass kernel instead of the two-pass kernels")
+    ap.add_argument("--ring-slots", type=int, default=0, help="one-pass ring slots (0: default)")
+    ap.add_argument("--no-other", action="store_true", help="skip timing the other MIXED kernel set")
+    ap.add_argument("--profile-case", choices=["mixed", "fp64"], default=None,
+                    help="run the small ncu profiling case instead of the benchmark")
+    ap.add_argument("--profile-steps", type=int, default=0)
     args = ap.parse_args()
 
     world = _env_int("WORLD_SIZE", 1)
@@ -309,8 +588,10 @@ def main():
         if out is not None:
             print(json.dumps(out), flush=True)
         return
+    if args.profile_case:
+        profile_case(args)
+        return
 
-    import numpy as np
     import torch
 
     import sympygr_b200 as sg
@@ -334,7 +615,8 @@ def main():
     rhs = torch.zeros_like(u)
     ctx = sg.Context(local_rank)
     stream = torch.cuda.ExternalStream(ctx.stream)
-    plans = {p: sg.Plan(ctx, blocks, p, args.chunk_points, args.slab_depth, args.deriv_ctas)
+    plans = {p: sg.Plan(ctx, blocks, p, args.chunk_points, args.slab_depth, args.deriv_ctas,
+                        single_pass=args.single_pass, ring_slots=args.ring_slots)
              for p in (sg.FP64, sg.MIXED)}
     params = {p: sg.Params.make(ko_sigma=SIGMA, precision=p) for p in (sg.FP64, sg.MIXED)}
     npts = plans[sg.FP64].points
@@ -367,6 +649,33 @@ def main():
     ms_mixed = timed(sg.MIXED, args.steps)
     clock_info = clocks.stop()
     ms_fp64 = timed(sg.FP64, args.steps)
+    for p in plans.values():
+        p.status()  # a bounded device wait that ran out would leave results incomplete
+
+    # the other MIXED kernel set on the same batch: the two-pass kernels (derivative
+    # scratch through HBM) or the one-pass kernel, whichever the headline did not use
+    mixed_other = None
+    if not args.no_other:
+        other_single = not plans[sg.MIXED].single_pass
+        p2 = sg.Plan(ctx, blocks, sg.MIXED, args.chunk_points, args.slab_depth, args.deriv_ctas,
+                     single_pass=other_single, ring_slots=args.ring_slots)
+        for _ in range(args.warmup):
+            p2.rhs_device(R, U, params[sg.MIXED])
+        barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            p2.rhs_device(R, U, params[sg.MIXED])
+        e1.record(stream)
+        e1.synchronize()
+        ms2 = max_over_ranks(e0.elapsed_time(e1), dist) / args.steps
+        d2, a2 = p2.profile(R, U, params[sg.MIXED])
+        p2.status()
+        p2.close()
+        mixed_other = {"kernels": "one-pass" if other_single else "two-pass",
+                       "value": round(sum_over_ranks(npts, dist) / (ms2 * 1e-3) / 1e6, 3),
+                       "ms_per_step": round(ms2, 3), "deriv_ms": round(d2, 3), "algebra_ms": round(a2, 3)}
 
     # accuracy of the headline path: mixed vs FP64 on the same inputs
     plans[sg.FP64].rhs_device(R, U, params[sg.FP64])
@@ -383,13 +692,11 @@ def main():
         per_var_rms.append(d.square().mean().sqrt().item() / rms_ref if rms_ref > 0 else 0.0)
         del d
     mixed_max_rel = max(per_var_max)
-    del ref64
 
     # per-kernel device time of one evaluation (events between launches)
     prof = {}
     for prec in (sg.MIXED, sg.FP64):
-        d_ms, a_ms = plans[prec].profile(R, U, params[prec])
-        prof[prec] = (d_ms, a_ms)
+        prof[prec] = plans[prec].profile(R, U, params[prec])
     peak64 = capi.fma_peak_tflops(local_rank, sg.FP64)
     peak32 = capi.fma_peak_tflops(local_rank, sg.MIXED)
 
@@ -424,88 +731,101 @@ def main():
     val_mixed = total_pts / (ms_mixed * 1e-3) / 1e6
     val_fp64 = total_pts / (ms_fp64 * 1e-3) / 1e6
 
-    d_ms, a_ms = prof[sg.MIXED]
-    alg_tf = ALGEBRA_FLOPS_PER_POINT * npts / (a_ms * 1e-3) / 1e12
-    d64, a64 = prof[sg.FP64]
-    alg64_tf = ALGEBRA_FLOPS_PER_POINT * npts / (a64 * 1e-3) / 1e12
     padded = sum(b.npad for b in blocks)
-    read_state = 24 * 8 * padded / npts
-    hbm_peak = None
+    read_state = BYTES_VARS * padded / npts
     try:
         with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as fh:
             hbm_peak = float(json.load(fh)["hbm_gbs"])
-        peak_src = "measured (MEASURED_PEAKS.json hbm_gbs, copy test)"
+        peak_src = "measured (hbm_gbs of the measured-peaks file, copy test)"
     except Exception:
         hbm_peak, peak_src = 6650.0, "fallback 6.65 TB/s"
-    nchunks = max(1, plans[sg.MIXED].launches // 3)  # 3 launches per chunk
+    rl = {}
+    for prec, mode in ((sg.MIXED, "mixed"), (sg.FP64, "fp64")):
+        d_ms, a_ms = prof[prec]
+        tr = NCU_TRAFFIC_PER_POINT[mode]
+        f32_alg = FLOPS_ALGEBRA if mode == "mixed" else 0
+        f64_alg = 0 if mode == "mixed" else FLOPS_ALGEBRA
+        if plans[prec].single_pass:
+            # one kernel per evaluation: its roofline is the evaluation's
+            one = roofline("bssn_fused_kernel<0> (one-pass: derivatives, algebra, KO, Sommerfeld)",
+                           d_ms, npts, read_state + BYTES_VARS, FLOPS_STENCIL, f32_alg, hbm_peak, peak64,
+                           peak32, tr.get("single_pass"), 1, peak_src)
+            ev = roofline(f"whole {mode} evaluation (all launches)", ms_mixed if mode == "mixed" else ms_fp64,
+                          npts, read_state + BYTES_VARS, FLOPS_STENCIL + f64_alg, f32_alg, hbm_peak, peak64,
+                          peak32, tr.get("single_pass"), 1, peak_src)
+            rl[mode] = {"single_pass": one, "evaluation": ev}
+            continue
+        nchunks = max(1, plans[prec].launches // 3)  # 3 launches per chunk
+        rl[mode] = {
+            # derivative stage: reads the state over the padded blocks; its scratch is
+            # not algorithmic (the reference's algorithm needs no scratch traffic)
+            "derivs": roofline(f"bssn_derivs_kind_kernel<{'float' if mode == 'mixed' else 'double'},*> (both kinds)",
+                               d_ms, npts, read_state, FLOPS_STENCIL, 0, hbm_peak, peak64, peak32,
+                               tr["derivs"], nchunks, peak_src),
+            # algebra: the state at the point in, the 24 right-hand sides out
+            "algebra": roofline(f"bssn_algebra_staged_kernel<{'float' if mode == 'mixed' else 'double'},0>",
+                                a_ms, npts, 2 * BYTES_VARS, f64_alg, f32_alg, hbm_peak, peak64, peak32,
+                                tr["algebra"], nchunks, peak_src),
+            "evaluation": roofline(f"whole {mode} evaluation (all launches)",
+                                   ms_mixed if mode == "mixed" else ms_fp64, npts,
+                                   read_state + BYTES_VARS, FLOPS_STENCIL + f64_alg, f32_alg,
+                                   hbm_peak, peak64, peak32, tr["derivs"] + tr["algebra"], 1, peak_src),
+        }
 
-    def hbm_roofline(kernel, ms, bytes_per_pt, mode, which):
-        gbs = bytes_per_pt * npts / (ms * 1e-3) / 1e9
-        traffic = NCU_TRAFFIC_PER_POINT[mode][which] * npts / nchunks
-        return {"kernel": kernel, "bound": "hbm", "achieved": round(gbs, 1), "peak": hbm_peak,
-                "unit": "GB/s", "frac": round(gbs / hbm_peak, 4), "traffic": round(traffic),
-                "bytes_per_point": round(bytes_per_pt, 1), "launches_per_step": nchunks,
-                "peak_source": peak_src,
-                "traffic_note": ("ncu DRAM bytes/point on a 3.15M-point case x points per chunk "
-                                 "(the derivative stage of a chunk is two launches, summed)")}
+    # the single-block configurations and the end-to-end legs run after the batch's
+    # device timing; the RHS of the FP64 path is kept for the reference check
+    single, single_inputs = (None, {})
+    if not args.no_single:
+        single, single_inputs = single_block_rates(ctx)
 
-    # end to end through the host API: H2D of the state, evaluate, D2H of the RHS.  Each
-    # rank pins a state and an RHS copy of its batch on the host; where the ranks on this
-    # node would need more than 60 % of its available memory, each times a
-    # class-proportional sample of its blocks instead (the metric is per point).
+    cpu, fp64_check = None, None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            frac = args.ref_fraction if args.ref_fraction > 0 else max(0.1, min(1.0, (os.cpu_count() or 1) / 30.0))
+            cpu, fp64_check = cpu_baseline_leg(u, blocks, ref64, single_inputs, frac)
+        except Exception as ex:  # the baseline is informational; never fail the bench on it
+            cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+                   "sample": f"failed: {ex}"}
+    del ref64
+
     e2e = None
     if not args.no_e2e:
-        local = max(1, _env_int("LOCAL_WORLD_SIZE", world))
-        span = max(b.offset + b.npad for b in blocks)
-        need = 2 * 24 * span * 8
-        budget = int(0.6 * host_bytes_available() / local)
-        hblocks, hplan, sample_note = blocks, plans[sg.MIXED], None
-        if need > budget:
-            sub = stratified_blocks(blocks, 0.9 * budget / need)
-            hblocks, off = [], 0
-            for b in sub:
-                hblocks.append(wl.Block(off, b.sz, b.bflag, b.pmin, b.pmax))
-                off += b.npad
-            u_h = torch.empty((24, off), dtype=u.dtype, pin_memory=True)
-            for b, hb in zip(sub, hblocks):
-                u_h[:, hb.offset:hb.offset + hb.npad].copy_(u[:, b.offset:b.offset + b.npad])
-            span = off
-            sample_note = (f"{len(hblocks)} of {len(blocks)} blocks per rank (class-proportional): "
-                           f"the full batch's host buffers ({need / 1e9:.1f} GB per rank) exceed "
-                           f"60 % of this node's available memory over {local} ranks")
-        else:
-            u_h = torch.empty(tuple(u.shape), dtype=u.dtype, pin_memory=True)
-            u_h.copy_(u)
+        u_h, hblocks, span, sample_note = e2e_leg(ctx, blocks, u, args, dist, world)
         del rhs, u
         U = R = None
         torch.cuda.empty_cache()
-        if sample_note:
-            hplan = sg.Plan(ctx, hblocks, sg.MIXED, args.chunk_points, args.slab_depth, args.deriv_ctas)
         e2e_pts = sum_over_ranks(sum(b.ninterior for b in hblocks), dist)
         r_h = torch.empty(tuple(u_h.shape), dtype=u_h.dtype, pin_memory=True)
-        p_host = sg.Params.make(ko_sigma=SIGMA, precision=sg.MIXED, ghost_policy=sg.GHOSTS_ZERO)
         UH, RH = [t.data_ptr() for t in u_h], [t.data_ptr() for t in r_h]
-        hplan.rhs_host(RH, UH, span, p_host)  # warm-up (allocates staging)
-        barrier()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(args.e2e_steps):
-            hplan.rhs_host(RH, UH, span, p_host)
-        e1.record(stream)
-        e1.synchronize()
-        ms = max_over_ranks(e0.elapsed_time(e1) / args.e2e_steps, dist)
         nbytes = 24 * span * 8
+        res = {}
+        for prec, name in ((sg.MIXED, "mixed"), (sg.FP64, "fp64")):
+            hplan = plans[prec] if sample_note is None else sg.Plan(ctx, hblocks, prec, args.chunk_points,
+                                                                     args.slab_depth, args.deriv_ctas)
+            p_host = sg.Params.make(ko_sigma=SIGMA, precision=prec, ghost_policy=sg.GHOSTS_ZERO)
+            hplan.rhs_host(RH, UH, span, p_host)  # warm-up (allocates staging)
+            barrier()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(args.e2e_steps):
+                hplan.rhs_host(RH, UH, span, p_host)
+            e1.record(stream)
+            e1.synchronize()
+            res[name] = max_over_ranks(e0.elapsed_time(e1) / args.e2e_steps, dist)
+            if sample_note is not None:
+                hplan.close()
         # the transfer bound: both directions' bytes at the concurrent copy rate
         gbs = duplex_copy_gbs(u_h, r_h)
         copy_ms = max_over_ranks(nbytes / (gbs * 1e9) * 1e3, dist)
-        if sample_note:
-            hplan.close()
         del u_h, r_h
+        ms = res["mixed"]
         e2e = {"value": round(e2e_pts / (ms * 1e-3) / 1e6, 3), "unit": UNIT,
                "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
                "ms_per_step": round(ms, 2), "steps": args.e2e_steps,
-               "api": "b200bssn_rhs_plan_host (pinned host arrays, ghosts zeroed)",
+               "api": "b200bssn_rhs_plan_host (pinned host arrays, ghosts zeroed), MIXED",
                "sample": sample_note,
+               "fp64": {"value": round(e2e_pts / (res["fp64"] * 1e-3) / 1e6, 3),
+                        "ms_per_step": round(res["fp64"], 2)},
                "copy_bound": {"duplex_gbs_per_direction": round(gbs, 1),
                               "ms_per_step": round(copy_ms, 2),
                               "value": round(e2e_pts / (copy_ms * 1e-3) / 1e6, 3),
@@ -513,58 +833,34 @@ def main():
                               "how": "1 GiB H2D and D2H copies at once from/to the same pinned "
                                      "arrays, one stream each; bytes per step / that rate"}}
 
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu:
-        try:
-            from oracle import pyoracle as po
-
-            if po.have_reference("fast"):
-                frac = ref_fraction(args)
-                sample = stratified_blocks(blocks, frac)
-                uh, sb = compact_host_batch(sample)
-                sb = [sb[i] for i in sorted(range(len(sb)), key=lambda i: -sb[i].npad)]
-                secs, pts = cpu_reference_run(uh, sb, os.cpu_count() or 1)
-                del uh
-                cpu = {"value": round(pts / secs / 1e6, 4), "unit": UNIT, "cores": os.cpu_count(),
-                       "kind": "reference",
-                       "sample": f"{len(sb)} blocks ({frac:.3g} class-proportional sample of the batch, "
-                                 f"{pts} interior points, largest first), one pass, {secs:.2f} s"}
-        except Exception as ex:  # the baseline is informational; never fail the bench on it
-            cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
-                   "sample": f"failed: {ex}"}
-
     if rank == 0:
+        d_ms, a_ms = prof[sg.MIXED]
+        d64, a64 = prof[sg.FP64]
         out = {
             "metric": METRIC, "value": round(val_mixed, 3), "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_mixed, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64 state+stencils / f32 algebra", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "blocks": len(blocks), "interior_points_per_gpu": npts,
-                       "l2": "inputs (26.7 GB per state) larger than L2; no flush",
-                       "scale": args.scale},
+            "config": workload_config(len(blocks), npts) if args.scale == 1.0 else
+            dict(workload_config(len(blocks), npts), scale=args.scale),
             "fp64": {"value": round(val_fp64, 3), "ms_per_step": round(ms_fp64, 3),
-                     "deriv_ms": round(d64, 3), "algebra_ms": round(a64, 3)},
+                     "deriv_ms": round(d64, 3), "algebra_ms": round(a64, 3),
+                     "vs_reference": fp64_check},
+            "mixed_kernels": "one-pass" if plans[sg.MIXED].single_pass else "two-pass",
+            "mixed_other_kernels": mixed_other,
             "mixed_vs_fp64": {"speedup": round(val_mixed / val_fp64, 3),
                               "max_rel_err": mixed_max_rel, "bar": MIXED_BAR,
                               "per_var_max_rel": [float(f"{x:.3g}") for x in per_var_max],
                               "per_var_rms_rel": [float(f"{x:.3g}") for x in per_var_rms]},
-            "kernels_ms": {"deriv": round(d_ms, 3), "algebra": round(a_ms, 3)},
-            # dominant kernel of the headline (mixed) evaluation: the derivative kernel
-            "roofline": hbm_roofline("bssn_derivs_kind_kernel<float,*> (both kinds)", d_ms,
-                                     read_state + SCRATCH_BYTES["mixed"], "mixed", 0),
-            "roofline_algebra": dict(
-                hbm_roofline("bssn_algebra_staged_kernel<float,0>", a_ms,
-                             24 * 8 + SCRATCH_BYTES["mixed"] + 24 * 8, "mixed", 1),
-                fp32_tflops=round(alg_tf, 3), fp32_peak=round(peak32, 2),
-                fp32_frac=round(alg_tf / peak32, 4), flops_per_point=ALGEBRA_FLOPS_PER_POINT,
-                fp_peak_source="measured FMA-chain microbenchmark (b200bssn_fma_peak)"),
-            "roofline_fp64": {
-                "derivs": hbm_roofline("bssn_derivs_kind_kernel<double,*> (both kinds)", d64,
-                                       read_state + SCRATCH_BYTES["fp64"], "fp64", 0),
-                "algebra": dict(hbm_roofline("bssn_algebra_staged_kernel<double,0>", a64,
-                                             24 * 8 + SCRATCH_BYTES["fp64"] + 24 * 8, "fp64", 1),
-                                fp64_tflops=round(alg64_tf, 3), fp64_peak=round(peak64, 2),
-                                fp64_frac=round(alg64_tf / peak64, 4))},
+            "kernels_ms": ({"single_pass": round(d_ms, 3)} if plans[sg.MIXED].single_pass
+                           else {"deriv": round(d_ms, 3), "algebra": round(a_ms, 3)}),
+            # dominant kernel of the headline (mixed) evaluation: the one-pass kernel (or,
+            # on the two-pass kernels, the derivative stage)
+            "roofline": rl["mixed"]["single_pass"] if plans[sg.MIXED].single_pass else rl["mixed"]["derivs"],
+            "roofline_algebra": rl["mixed"].get("algebra"),
+            "roofline_evaluation": rl["mixed"]["evaluation"],
+            "roofline_fp64": rl["fp64"],
+            "single_block": single,
             "upwind_mode": upwind,
             "gpu_launches": launches,
             "clocks": clock_info,

@@ -109,7 +109,7 @@ int b200bssn_rhs(b200bssn_ctx *ctx, double *const *rhs, const double *const *u,
 /* Work plan for a fixed block list: descriptors, tiles and the derivative
  * scratch live on the device.  Build once, evaluate many times (RK stages).
  * `chunk_points` bounds the interior points evaluated per kernel pair (and so the
- * scratch: 1296 bytes per point in FP64, 744 in MIXED); 0 picks the default. */
+ * scratch: 1296 bytes per point in FP64, 648 in MIXED); 0 picks the default. */
 int b200bssn_plan_create(b200bssn_ctx *ctx, const b200bssn_block *blocks, uint32_t nblocks,
                          uint32_t precision, uint64_t chunk_points, b200bssn_plan **plan);
 int b200bssn_plan_destroy(b200bssn_plan *plan);
@@ -128,6 +128,14 @@ typedef struct b200bssn_plan_options {
    * upwind stencils deriv42adv_* (bssn/src/derivs.cpp:495-900), upwinded by the sign
    * of the matching shift component; the scratch grows by 72 slots per point. */
   uint32_t advective;
+  /* 1: a MIXED plan with centred advection evaluates the right-hand side (and RK4
+   * stages) in one pass -- one persistent kernel over every block, its derivative
+   * scratch in an L2-sized ring of tile-slab slots -- instead of the two-pass
+   * kernels (derivative scratch through HBM).  FP64, the upwind mode, the
+   * constraints and the host-array path always use the two-pass kernels. */
+  uint32_t single_pass;
+  /* Ring slots of the one-pass kernel (0: 32; each slot 3072 points, 2 MB). */
+  uint32_t ring_slots;
 } b200bssn_plan_options;
 
 /* b200bssn_plan_create with explicit options (opts may be NULL). */
@@ -138,6 +146,12 @@ int b200bssn_plan_create_ex(b200bssn_ctx *ctx, const b200bssn_block *blocks, uin
  * evaluation issues. */
 uint64_t b200bssn_plan_points(const b200bssn_plan *plan);
 uint32_t b200bssn_plan_launches(const b200bssn_plan *plan);
+/* 1 when the plan's right-hand side runs as the one-pass kernel, else 0. */
+uint32_t b200bssn_plan_single_pass(const b200bssn_plan *plan);
+/* Synchronises the context and reads the plan's device error word: B200BSSN_OK, or
+ * B200BSSN_ERR_TIMEOUT when a bounded wait of the one-pass kernel ran out during
+ * the last evaluation (its results are then incomplete). */
+int b200bssn_plan_status(b200bssn_plan *plan);
 
 /* Batched right-hand side on DEVICE arrays (the bssnRHS block loop,
  * bssn/src/rhs.cpp:41-68).  rhs_dev[v]/u_dev[v] are device pointers to the
@@ -250,7 +264,9 @@ uint32_t b200bssn_rk4_graph_steps(const b200bssn_rk4 *rk);
  * overlap on the GPU race and corrupt each other, so serialise them per device.
  * The first call on a device looks up the array's address (cudaGetSymbolAddress)
  * and sets a kernel attribute with that device current; make it before any stream
- * capture.  Asynchronous on `stream` (NULL: the legacy default stream). */
+ * capture.  That address is kept for the life of the process: calls after a
+ * cudaDeviceReset of the device are not supported.  Asynchronous on `stream` (NULL:
+ * the legacy default stream). */
 int b200bssn_rhs_noalloc(double *const *rhs_dev, const double *const *u_dev,
                          const b200bssn_block *block, const b200bssn_params *prm,
                          void *stream);

@@ -20,7 +20,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_LIB = os.path.join(HERE, "_build", "libbssn_oracle.so")
 REF_PARITY = os.path.join(HERE, "_ref", "libbssn_ref_parity.so")
-REF_FAST = os.path.join(HERE, "_ref", "libbssn_ref_fast.so")
+REF_FAST = os.path.join(HERE, "_ref", "libbssn_ref_fast.so")        # -march=x86-64-v3
+REF_FAST_V4 = os.path.join(HERE, "_ref", "libbssn_ref_fast_v4.so")  # -march=x86-64-v4
 NUM_VARS = 24
 NUM_DERIVS = 138
 NUM_SLOTS = 162
@@ -49,14 +50,27 @@ def params(lambda_=(1, 1, 1, 1), lambda_f=(1.0, 0.0), eta_const=2.0, eta_r0=50.0
     return p
 
 
+def reference_checkout() -> str | None:
+    """The reference checkout: $SYMPYGR_REFERENCE, else a ``reference`` folder beside
+    this repository; None when neither holds bssn/src."""
+    cands = [os.environ.get("SYMPYGR_REFERENCE"),
+             os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference")]
+    for c in cands:
+        if c and os.path.isdir(os.path.join(c, "bssn", "src")):
+            return os.path.abspath(c)
+    return None
+
+
 def build(with_reference: bool | None = None):
-    """make -C oracle (the reference flavours only where the reference tree exists)."""
+    """make -C oracle (the reference flavours only where the reference checkout exists)."""
     targets = ["oracle"]
+    ref = reference_checkout()
     if with_reference is None:
-        with_reference = os.path.isdir("/root/reference/bssn")
+        with_reference = ref is not None
     if with_reference:
         targets.append("ref")
-    subprocess.run(["make", "-s", "-C", HERE, *targets], check=True)
+    extra = [f"SYMPYGR_REFERENCE={ref}"] if ref else []
+    subprocess.run(["make", "-s", "-C", HERE, *extra, *targets], check=True)
 
 
 def _load(path):
@@ -73,8 +87,29 @@ def oracle_lib():
     return _load(ORACLE_LIB)
 
 
+def _cpu_has_avx512() -> bool:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("flags"):
+                    fl = set(line.split(":", 1)[1].split())
+                    return {"avx512f", "avx512dq", "avx512cd", "avx512bw", "avx512vl"} <= fl
+    except OSError:
+        pass
+    return False
+
+
+def fast_flavour_path() -> str:
+    """The timing build for this CPU: x86-64-v4 (AVX-512) where the CPU has it and the
+    build exists, else x86-64-v3 -- the closest stand-in for -march=native available
+    on a host without the reference sources."""
+    if _cpu_has_avx512() and os.path.exists(REF_FAST_V4):
+        return REF_FAST_V4
+    return REF_FAST
+
+
 def have_reference(flavour="parity") -> bool:
-    return os.path.exists(REF_PARITY if flavour == "parity" else REF_FAST)
+    return os.path.exists(REF_PARITY if flavour == "parity" else fast_flavour_path())
 
 
 def _ptrs(arr2d, offset=0):
@@ -214,7 +249,7 @@ class OracleRK4:
 
 
 def _ref(flavour):
-    lib = _load(REF_PARITY if flavour == "parity" else REF_FAST)
+    lib = _load(REF_PARITY if flavour == "parity" else fast_flavour_path())
     lib.ref_bssnrhs_blocks_omp.restype = ctypes.c_double
     return lib
 
@@ -347,3 +382,26 @@ def rel_errors(got, ref):
     scale = np.maximum(np.abs(ref).max(axis=1), 1e-300)
     rms_scale = np.maximum(np.sqrt((ref ** 2).mean(axis=1)), 1e-300)
     return np.abs(d).max(axis=1) / scale, np.sqrt((d ** 2).mean(axis=1)) / rms_scale
+
+
+def batch_rel_errors(pairs, noise=1e-10):
+    """MIXED-path norms over several blocks: `pairs` is a list of (got, ref) arrays of
+    shape [nv, points] (one per block).  Returns (over_batch, per_block):
+
+    * over_batch[v] = max over blocks of max|g - r| / max over blocks of max|r| -- the
+      norm the benchmark reports for a whole batch;
+    * per_block[k][v] = max|g - r| / max|r| on block k, where a variable whose largest
+      |r| on that block is below `noise` times the block's largest |r| over all
+      variables (a right-hand side that vanishes there up to rounding) is measured
+      against that block scale instead.
+    """
+    nv = pairs[0][1].shape[0]
+    dmax, rmax, per_block = np.zeros(nv), np.zeros(nv), []
+    for got, ref in pairs:
+        d = np.abs(np.asarray(got) - np.asarray(ref)).max(axis=1)
+        r = np.abs(np.asarray(ref)).max(axis=1)
+        dmax, rmax = np.maximum(dmax, d), np.maximum(rmax, r)
+        scale = np.maximum(r, noise * r.max())
+        per_block.append(d / np.maximum(scale, 1e-300))
+    return dmax / np.maximum(rmax, 1e-300), per_block
+

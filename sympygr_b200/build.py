@@ -18,7 +18,7 @@ LIBDIR = os.path.join(PKG, "lib")
 LIB = os.path.join(LIBDIR, "libb200bssn.so")
 
 SOURCES = ["b200bssn.cu", "diagnostics.cu", "noalloc.cu", "rk4.cu", "guard.cu"]
-HEADERS = ["rhs_kernels.cuh", "stencils.cuh", "plan_types.h", "plan_internal.h", "constraint_kernels.cuh",
+HEADERS = ["rhs_kernels.cuh", "fused_kernel.cuh", "stencils.cuh", "plan_types.h", "plan_internal.h", "constraint_kernels.cuh",
            "generated/bssn_rhs_algebra.cuh", "generated/bssn_rhs_algebra_adv.cuh",
            "generated/bssn_constraints_algebra.cuh"]
 

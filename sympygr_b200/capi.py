@@ -93,6 +93,8 @@ class PlanOptions(ctypes.Structure):
         ("deriv_ctas_per_sm", ctypes.c_uint32),
         ("block_slab_depth", ctypes.POINTER(ctypes.c_uint32)),
         ("advective", ctypes.c_uint32),
+        ("single_pass", ctypes.c_uint32),
+        ("ring_slots", ctypes.c_uint32),
     ]
 
 
@@ -118,6 +120,8 @@ SIGNATURES = [
     ("b200bssn_plan_destroy", ctypes.c_int, [_P]),
     ("b200bssn_plan_points", ctypes.c_uint64, [_P]),
     ("b200bssn_plan_launches", ctypes.c_uint32, [_P]),
+    ("b200bssn_plan_single_pass", ctypes.c_uint32, [_P]),
+    ("b200bssn_plan_status", ctypes.c_int, [_P]),
     ("b200bssn_rhs_plan_device", ctypes.c_int, [_P, _P, _P, ctypes.POINTER(Params), _P]),
     ("b200bssn_rhs_plan_host", ctypes.c_int, [_P, _P, _P, ctypes.c_uint64, ctypes.POINTER(Params)]),
     ("b200bssn_plan_profile", ctypes.c_int, [_P, _P, _P, ctypes.POINTER(Params),
@@ -282,7 +286,8 @@ class Plan:
 
     def __init__(self, ctx: Context, blocks: Sequence[Block], precision: int = FP64,
                  chunk_points: int = 0, slab_depth: int = 0, deriv_ctas_per_sm: int = 0,
-                 block_slab_depth: Sequence[int] | None = None, advective: bool = False):
+                 block_slab_depth: Sequence[int] | None = None, advective: bool = False,
+                 single_pass: bool = False, ring_slots: int = 0):
         lib = load()
         arr = (BlockC * len(blocks))()
         for i, b in enumerate(blocks):
@@ -295,6 +300,8 @@ class Plan:
         h = ctypes.c_void_p()
         opts = PlanOptions(chunk_points, slab_depth, deriv_ctas_per_sm)
         opts.advective = 1 if advective else 0
+        opts.single_pass = 1 if single_pass else 0
+        opts.ring_slots = int(ring_slots)
         if block_slab_depth is not None:
             if len(block_slab_depth) != len(blocks):
                 raise ValueError("block_slab_depth needs one entry per block")
@@ -315,6 +322,15 @@ class Plan:
     @property
     def launches(self) -> int:
         return int(load().b200bssn_plan_launches(self.handle))
+
+    @property
+    def single_pass(self) -> bool:
+        """True when the right-hand side runs as the one-pass kernel."""
+        return bool(load().b200bssn_plan_single_pass(self.handle))
+
+    def status(self):
+        """Synchronise and raise if a bounded device wait of the last evaluation ran out."""
+        _check(load().b200bssn_plan_status(self.handle), "b200bssn_plan_status", self.ctx)
 
     def rhs_device(self, rhs, u, params: Params, stream: int = 0):
         """Batched RHS on device arrays (torch CUDA tensors or raw pointers);

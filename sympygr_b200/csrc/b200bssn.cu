@@ -10,6 +10,7 @@
 
 #include "b200bssn.h"
 #include "constraint_kernels.cuh"
+#include "fused_kernel.cuh"
 #include "plan_internal.h"
 #include "rhs_kernels.cuh"
 
@@ -170,7 +171,50 @@ int enqueue_chunk(b200bssn_plan* P, DerivArgs da, AlgebraArgs aa, size_t ci, int
   return B200BSSN_OK;
 }
 
+// One evaluation as the one-pass kernel: zero the sync words, then one launch over
+// every tile-slab of the plan.  With `ev` non-null, events ev[0], ev[1] around it.
+int launch_single_pass(b200bssn_plan* P, const DerivArgs& da, const AlgebraArgs& aa, cudaStream_t s,
+                       cudaEvent_t* ev) {
+  b200bssn_ctx* ctx = P->ctx;
+  FusedArgs f;
+  std::memset(&f, 0, sizeof(f));
+  f.d = da;
+  f.a = aa;
+  f.d.dscr = P->fring_d;
+  f.d.koscr = P->fring_k;
+  f.d.cap = P->nring * kFusedSlotPts;
+  f.tiles = P->d_ftiles;
+  f.group_tile = P->d_group_tile;
+  f.ntiles = (int32_t)P->ftiles.size();
+  f.ngroups = P->ngroups;
+  f.nring = P->nring;
+  f.sync = P->d_fsync;
+  CK(ctx, cudaMemsetAsync(P->d_fsync, 0, P->fsync_words * sizeof(int), s));
+  if (ev) CK(ctx, cudaEventRecord(ev[0], s));
+  const unsigned grid = (unsigned)P->fused_grid;
+  switch (aa.rk.mode) {
+    case RK_FIRST:
+      bssn_fused_kernel<RK_FIRST><<<grid, kFusedThreads, kFusedSmemBytes, s>>>(f);
+      break;
+    case RK_MIDDLE:
+      bssn_fused_kernel<RK_MIDDLE><<<grid, kFusedThreads, kFusedSmemBytes, s>>>(f);
+      break;
+    case RK_LAST:
+      bssn_fused_kernel<RK_LAST><<<grid, kFusedThreads, kFusedSmemBytes, s>>>(f);
+      break;
+    default:
+      bssn_fused_kernel<RK_NONE><<<grid, kFusedThreads, kFusedSmemBytes, s>>>(f);
+      break;
+  }
+  CK(ctx, cudaGetLastError());
+  if (ev) CK(ctx, cudaEventRecord(ev[1], s));
+  return B200BSSN_OK;
+}
+
 // Enqueues one evaluation of the plan.
+//
+// One-pass plans (MIXED, centred advection) run the right-hand side and the RK4
+// stages as launch_single_pass; the constraints always take the two-pass kernels.
 //
 // With `ev` null and more than one chunk the chunks are pipelined over two
 // internal streams: the derivative kernel of chunk c (stream s_deriv, scratch
@@ -194,6 +238,7 @@ int b200bssn::host::launch_plan(b200bssn_plan* P, double* const* rhs, const doub
   AlgebraArgs aa;
   make_args(P, rhs, u, prm, da, aa);
   if (rk) aa.rk = *rk;
+  if (P->single_pass && !ca) return launch_single_pass(P, da, aa, s, ev);
   const size_t nch = P->chunks.size();
   const bool pipelined = ev == nullptr && nch > 1;
   cudaStream_t s1 = pipelined ? ctx->s_deriv : s, s2 = pipelined ? ctx->s_alg : s;
@@ -224,6 +269,11 @@ int set_kernel_attributes(b200bssn_ctx* ctx) {
                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDerivSmemBytes));
   CK(ctx, cudaFuncSetAttribute(bssn_derivs_kernel<float>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDerivSmemBytes));
+  const int fb = (int)kFusedSmemBytes;
+  CK(ctx, cudaFuncSetAttribute(bssn_fused_kernel<RK_NONE>, cudaFuncAttributeMaxDynamicSharedMemorySize, fb));
+  CK(ctx, cudaFuncSetAttribute(bssn_fused_kernel<RK_FIRST>, cudaFuncAttributeMaxDynamicSharedMemorySize, fb));
+  CK(ctx, cudaFuncSetAttribute(bssn_fused_kernel<RK_MIDDLE>, cudaFuncAttributeMaxDynamicSharedMemorySize, fb));
+  CK(ctx, cudaFuncSetAttribute(bssn_fused_kernel<RK_LAST>, cudaFuncAttributeMaxDynamicSharedMemorySize, fb));
   return B200BSSN_OK;
 }
 
@@ -510,6 +560,58 @@ int b200bssn_plan_create_ex(b200bssn_ctx* ctx, const b200bssn_block* blocks, uin
     P->alg_grid = std::max(1, sms * std::max(1, alg_per_sm));
   }
 
+  // one-pass path (when asked for): MIXED with centred advection.  Tile-slabs of the
+  // largest blocks first (the launch ends on small items); within a block, slab by
+  // slab and tile by tile, so neighbouring items share halos.
+  P->single_pass = precision == B200BSSN_MIXED && !P->advective && o.single_pass;
+  if (P->single_pass) {
+    P->nring = o.ring_slots ? (int32_t)std::min<uint32_t>(o.ring_slots, 1024) : kFusedRingDefault;
+    std::vector<uint32_t> order(nblocks);
+    for (uint32_t b = 0; b < nblocks; ++b) order[b] = b;
+    auto npad = [&](uint32_t b) {
+      const BlockDev& B = P->blocks[b];
+      return (int64_t)B.sz[0] * B.sz[1] * B.sz[2];
+    };
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) { return npad(x) > npad(y); });
+    int64_t groups = 0;
+    for (uint32_t b : order) {
+      const BlockDev& B = P->blocks[b];
+      const int I0 = B.sz[0] - 6, I1 = B.sz[1] - 6, I2 = B.sz[2] - 6;
+      const int nslab = (I2 + kFusedSlab - 1) / kFusedSlab;
+      for (int sl = 0; sl < nslab; ++sl) {
+        const int k0 = (int)((int64_t)sl * I2 / nslab), k1 = (int)((int64_t)(sl + 1) * I2 / nslab);
+        for (int j0 = 0; j0 < I1; j0 += kTileY)
+          for (int i0 = 0; i0 < I0; i0 += kTileX) {
+            FusedTileDev t;
+            t.block = (int32_t)b;
+            t.i0 = (int16_t)i0;
+            t.j0 = (int16_t)j0;
+            t.ex = (int16_t)std::min(kTileX, I0 - i0);
+            t.ey = (int16_t)std::min(kTileY, I1 - j0);
+            t.k0 = (int16_t)k0;
+            t.nz = (int16_t)(k1 - k0);
+            t.group_base = (int32_t)std::min<int64_t>(groups, INT32_MAX);
+            groups += t.nz;
+            P->ftiles.push_back(t);
+          }
+      }
+    }
+    if (groups >= INT32_MAX || (int64_t)P->ftiles.size() * kNumVars >= INT32_MAX) {
+      delete P;
+      return B200BSSN_ERR_SIZE_LIMIT;
+    }
+    P->ngroups = (int32_t)groups;
+    P->group_tile.resize((size_t)groups);
+    for (size_t t = 0; t < P->ftiles.size(); ++t)
+      for (int z = 0; z < P->ftiles[t].nz; ++z) P->group_tile[(size_t)P->ftiles[t].group_base + z] = (int32_t)t;
+    P->fsync_words = 4 + 2 * P->ftiles.size() + (size_t)P->nring;
+    int sms = 0, per_sm = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bssn_fused_kernel<RK_NONE>, kFusedThreads,
+                                                  kFusedSmemBytes);
+    P->fused_grid = std::max(1, sms * std::max(1, per_sm));
+  }
+
   const size_t nb = P->blocks.size() * sizeof(BlockDev), nu = P->units.size() * sizeof(UnitDev),
                nt = P->tiles.size() * sizeof(TileDev), nr = P->ranges.size() * sizeof(RangeDev);
   auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
@@ -522,6 +624,24 @@ int b200bssn_plan_create_ex(b200bssn_ctx* ctx, const b200bssn_block* blocks, uin
     // 16-byte chunks or 32-point columns and may read past the last run's end
     e = cudaMalloc(&P->dscr[b], (size_t)nslots * P->cap * st + 512);
     if (e == cudaSuccess) e = cudaMalloc(&P->koscr[b], (size_t)kNumVars * P->cap * st + 512);
+  }
+  if (e == cudaSuccess && P->single_pass) {
+    const size_t ntb = al(P->ftiles.size() * sizeof(FusedTileDev)), ngb = al(P->group_tile.size() * sizeof(int32_t));
+    e = cudaMalloc(&P->fdesc, ntb + ngb + al(P->fsync_words * sizeof(int)));
+    if (e == cudaSuccess) {
+      char* fb = static_cast<char*>(P->fdesc);
+      P->d_ftiles = reinterpret_cast<FusedTileDev*>(fb);
+      P->d_group_tile = reinterpret_cast<int32_t*>(fb + ntb);
+      P->d_fsync = reinterpret_cast<int*>(fb + ntb + ngb);
+      e = cudaMemcpy(P->d_ftiles, P->ftiles.data(), P->ftiles.size() * sizeof(FusedTileDev),
+                     cudaMemcpyHostToDevice);
+    }
+    if (e == cudaSuccess)
+      e = cudaMemcpy(P->d_group_tile, P->group_tile.data(), P->group_tile.size() * sizeof(int32_t),
+                     cudaMemcpyHostToDevice);
+    const size_t ring_pts = (size_t)P->nring * kFusedSlotPts;
+    if (e == cudaSuccess) e = cudaMalloc(&P->fring_d, ring_pts * kNumDerivs * sizeof(float) + 512);
+    if (e == cudaSuccess) e = cudaMalloc(&P->fring_k, ring_pts * kNumVars * sizeof(float) + 512);
   }
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&P->ev_fork, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaMalloc((void**)&P->d_counters, 2 * P->chunks.size() * sizeof(int));
@@ -579,6 +699,9 @@ int b200bssn_plan_destroy(b200bssn_plan* P) {
   if (P->ev_fork) cudaEventDestroy(P->ev_fork);
   cudaFree(P->d_counters);
   cudaFree(P->d_guard);
+  cudaFree(P->fdesc);
+  cudaFree(P->fring_d);
+  cudaFree(P->fring_k);
   cudaFree(P->st_u);
   cudaFree(P->st_rhs);
   delete P;
@@ -588,7 +711,26 @@ int b200bssn_plan_destroy(b200bssn_plan* P) {
 uint64_t b200bssn_plan_points(const b200bssn_plan* P) { return P ? P->points : 0; }
 
 uint32_t b200bssn_plan_launches(const b200bssn_plan* P) {
-  return P ? (uint32_t)(3 * P->chunks.size()) : 0;  // two derivative kernels + algebra
+  if (!P) return 0;
+  if (P->single_pass) return 1;                 // the one-pass kernel
+  return (uint32_t)(3 * P->chunks.size());      // two derivative kernels + algebra per chunk
+}
+
+uint32_t b200bssn_plan_single_pass(const b200bssn_plan* P) { return P && P->single_pass ? 1u : 0u; }
+
+int b200bssn_plan_status(b200bssn_plan* P) {
+  if (!P) return B200BSSN_ERR_INVALID_ARGUMENT;
+  b200bssn_ctx* ctx = P->ctx;
+  CK(ctx, cudaSetDevice(ctx->device));
+  CK(ctx, cudaDeviceSynchronize());
+  if (!P->single_pass) return B200BSSN_OK;
+  int err = 0;
+  CK(ctx, cudaMemcpy(&err, P->d_fsync + 2, sizeof(int), cudaMemcpyDeviceToHost));
+  if (err) {
+    ctx->last_error = "one-pass kernel: a bounded wait for work timed out";
+    return B200BSSN_ERR_TIMEOUT;
+  }
+  return B200BSSN_OK;
 }
 
 int b200bssn_rhs_plan_device(b200bssn_plan* P, double* const* rhs_dev, const double* const* u_dev,
@@ -609,6 +751,24 @@ int b200bssn_plan_profile(b200bssn_plan* P, double* const* rhs_dev, const double
   if (prm->precision != P->precision) return B200BSSN_ERR_INVALID_ARGUMENT;
   b200bssn_ctx* ctx = P->ctx;
   CK(ctx, cudaSetDevice(ctx->device));
+  if (P->single_pass) {
+    // one kernel: its whole time is reported as the derivative part, 0 as the algebra
+    cudaEvent_t ev[2];
+    CK(ctx, cudaEventCreate(&ev[0]));
+    CK(ctx, cudaEventCreate(&ev[1]));
+    int rc = launch_plan(P, rhs_dev, u_dev, prm, ctx->stream, ev);
+    float t = 0;
+    if (rc == B200BSSN_OK) {
+      cudaError_t e = cudaStreamSynchronize(ctx->stream);
+      if (e != cudaSuccess) rc = fail_cuda(ctx, e, "profile sync");
+      else cudaEventElapsedTime(&t, ev[0], ev[1]);
+    }
+    cudaEventDestroy(ev[0]);
+    cudaEventDestroy(ev[1]);
+    *ms_deriv = t;
+    *ms_algebra = 0.0;
+    return rc;
+  }
   std::vector<cudaEvent_t> ev(4 * P->chunks.size());
   for (auto& e : ev) CK(ctx, cudaEventCreate(&e));
   int rc = launch_plan(P, rhs_dev, u_dev, prm, ctx->stream, ev.data());
@@ -891,7 +1051,7 @@ int b200bssn_constraints_plan_device(b200bssn_plan* P, double* const* con_dev,
 int b200bssn_debug_block_scratch(b200bssn_ctx* ctx, double* slots, uint64_t npts) {
   if (!ctx || !slots || !ctx->blk_plan) return B200BSSN_ERR_INVALID_ARGUMENT;
   b200bssn_plan* P = ctx->blk_plan;
-  if (P->chunks.size() != 1 || npts != P->points) return B200BSSN_ERR_INVALID_ARGUMENT;
+  if (P->single_pass || P->chunks.size() != 1 || npts != P->points) return B200BSSN_ERR_INVALID_ARGUMENT;
   CK(ctx, cudaSetDevice(ctx->device));
   CK(ctx, cudaStreamSynchronize(ctx->stream));
   // the scratch is blocked by 32 points (scr_index): copy it whole, then gather

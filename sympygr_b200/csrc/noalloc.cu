@@ -20,8 +20,15 @@
 //    streams, or host threads racing) overwrite each other's scratch and give
 //    wrong results.  Serialise calls per device;
 //  * the first call on each device looks up the array's device address with
-//    cudaGetSymbolAddress and sets the derivative kernel's shared-memory limit,
-//    with that device current; make that first call before any stream capture.
+//    cudaGetSymbolAddress, sets the derivative kernel's shared-memory limit and
+//    reads its occupancy, with that device current; make that first call before any
+//    stream capture.  The address is kept for the life of the process, so calls after
+//    a cudaDeviceReset of that device (which reloads the library's device code at a
+//    new address) are not supported.
+//
+// The derivative kernel here is the combined one over all 24 variables
+// (bssn_derivs_kernel), which only this entry point launches; the plans use the two
+// per-kind kernels.
 #include <cuda_runtime.h>
 
 #include <cstring>
@@ -56,14 +63,18 @@ constexpr size_t kNoallocBytes = kOffKo + al256(sizeof(double) * kNumVars * kNoa
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocBytes];
 
-// Per-device address of g_noalloc_scratch (host-side handle -> device address).
+// Per-device address of g_noalloc_scratch (host-side handle -> device address) and
+// the resident CTA count of the persistent derivative kernel, per precision.
 std::mutex g_setup_mutex;
 void* g_scratch_addr[kMaxDevices] = {};
+int g_deriv_grid[kMaxDevices][2] = {};  // [dev][0: FP64, 1: MIXED]
 
-int setup_device(int dev, void** addr) {
+int setup_device(int dev, void** addr, int* grid64, int* grid32) {
   std::lock_guard<std::mutex> lock(g_setup_mutex);
   if (g_scratch_addr[dev]) {
     *addr = g_scratch_addr[dev];
+    *grid64 = g_deriv_grid[dev][0];
+    *grid32 = g_deriv_grid[dev][1];
     return B200BSSN_OK;
   }
   void* p = nullptr;
@@ -78,8 +89,24 @@ int setup_device(int dev, void** addr) {
     cudaGetLastError();
     return B200BSSN_ERR_CUDA;
   }
+  // the derivative kernel is persistent (each CTA pulls items from the work counter),
+  // so its grid is the CTAs that fit on the GPU at once, as the plans size it
+  int sms = 0, occ64 = 0, occ32 = 0;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ64, bssn_derivs_kernel<double>, kDerivThreads,
+                                                    kDerivSmemBytes) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ32, bssn_derivs_kernel<float>, kDerivThreads,
+                                                    kDerivSmemBytes) != cudaSuccess ||
+      sms <= 0 || occ64 <= 0 || occ32 <= 0) {
+    cudaGetLastError();
+    return B200BSSN_ERR_CUDA;
+  }
+  g_deriv_grid[dev][0] = sms * occ64;
+  g_deriv_grid[dev][1] = sms * occ32;
   g_scratch_addr[dev] = p;
   *addr = p;
+  *grid64 = g_deriv_grid[dev][0];
+  *grid32 = g_deriv_grid[dev][1];
   return B200BSSN_OK;
 }
 
@@ -154,7 +181,8 @@ extern "C" int b200bssn_rhs_noalloc(double* const* rhs_dev, const double* const*
     return B200BSSN_ERR_NO_DEVICE;
   }
   void* base = nullptr;
-  int rc = setup_device(dev, &base);
+  int grid64 = 0, grid32 = 0;
+  int rc = setup_device(dev, &base, &grid64, &grid32);
   if (rc != B200BSSN_OK) return rc;
   char* b = static_cast<char*>(base);
   UnitDev* units = reinterpret_cast<UnitDev*>(b + kOffUnits);
@@ -209,7 +237,9 @@ extern "C" int b200bssn_rhs_noalloc(double* const* rhs_dev, const double* const*
   aa.eta_damping_exp = prm->eta_damping_exp;
   aa.ko_sigma = prm->ko_sigma;
 
-  const dim3 g1((unsigned)(n_units * tiles_x * tiles_y * kNumVars), 1);
+  const int64_t items = n_units * tiles_x * tiles_y * kNumVars;
+  const int64_t gmax = prm->precision == B200BSSN_MIXED ? grid32 : grid64;
+  const dim3 g1((unsigned)(items < gmax ? items : gmax), 1);
   const unsigned g2 = (unsigned)(n_units * rpu);  // runs past a unit's end have count 0
   if (prm->precision == B200BSSN_MIXED) {
     bssn_derivs_kernel<float><<<g1, kDerivThreads, kDerivSmemBytes, s>>>(da);

@@ -75,6 +75,19 @@ struct b200bssn_plan {
   std::vector<cudaEvent_t> ev_in;  // per chunk: upload done
   int deriv_grid[2] = {0, 0};  // resident CTAs of the two persistent derivative kernels
   int alg_grid = 0;           // resident CTAs of the persistent staged algebra kernel (MIXED)
+  // one-pass path (MIXED, centred advection): tile-slabs in launch order, the tile-slab
+  // of every algebra group, the per-evaluation sync words and the scratch ring
+  bool single_pass = false;
+  int32_t nring = 0, ngroups = 0, fused_grid = 0;
+  std::vector<b200bssn::FusedTileDev> ftiles;
+  std::vector<int32_t> group_tile;
+  void* fdesc = nullptr;
+  b200bssn::FusedTileDev* d_ftiles = nullptr;
+  int32_t* d_group_tile = nullptr;
+  int* d_fsync = nullptr;
+  size_t fsync_words = 0;
+  void* fring_d = nullptr;  // nring * kFusedSlotPts points x 138 slots (float)
+  void* fring_k = nullptr;  // nring * kFusedSlotPts points x 24 KO sums (float)
   // host-batch staging (allocated on first host call)
   double* st_u = nullptr;
   double* st_rhs = nullptr;

@@ -42,6 +42,19 @@ struct TileDev {
   int16_t ex, ey;    // extents (<= kTileX, kTileY)
 };
 
+// One tile-slab of the one-pass kernel: a 16x8 column tile of a block over a z-slab
+// of at most kFusedSlab interior planes.
+struct FusedTileDev {
+  int32_t block;
+  int16_t i0, j0;     // interior-relative x-y origin of the tile
+  int16_t ex, ey;     // extents (<= kTileX, kTileY)
+  int16_t k0, nz;     // interior-relative first plane and planes (<= kFusedSlab)
+  int32_t group_base; // first algebra group of the tile-slab (one group per plane)
+};
+constexpr int kFusedSlab = 24;                               // max interior planes per tile-slab
+constexpr int kFusedSlotPts = kTileX * kTileY * kFusedSlab;  // 3072 points per ring slot
+constexpr int kFusedRingDefault = 32;                        // slots: 64 MB in MIXED
+
 struct RangeDev {
   int32_t unit;
   int32_t start;     // first compact point index within the unit

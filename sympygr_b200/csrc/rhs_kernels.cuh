@@ -391,17 +391,23 @@ struct RowsFor<float> { using type = SplitRows; };
 // by the sign of the matching shift component at the point); CL: some point of the
 // item takes a closure row (tile_has_closure) -- without, the closure branches and
 // the face cases of the upwind rows compile away.
+//
+// Scratch point of output (tile column tx, ty; plane zo of the slab): lp = col_base +
+// tx + row_stride * ty + plane_pts * zo -- the unit's compact numbering on the two-pass
+// path, the tile's own 16x8-per-plane numbering inside a ring slot on the single-pass path.
+struct ScratchMap {
+  int32_t col_base, row_stride, plane_pts;
+};
+
 template <typename ST, bool DD, bool ADV = false, bool CL = true>
-__device__ __forceinline__ void derive_tile(const DerivArgs& a, const TileDev t, const int v,
-                                            double (*s_plane)[kPlane], void* s_dxp_raw,
-                                            double* s_kq, LineScales* s_sc) {
+__device__ __forceinline__ void derive_item(const DerivArgs& a, const UnitDev& un, const TileDev& t,
+                                            const ScratchMap sm, const int v, double (*s_plane)[kPlane],
+                                            void* s_dxp_raw, double* s_kq, LineScales* s_sc) {
   using Rows = typename RowsFor<ST>::type;
   constexpr int NS = ADV ? kNumDerivs + 3 * kNumVars : kNumDerivs;  // slots per point
   double* s_dxp = static_cast<double*>(s_dxp_raw);
-  const UnitDev un = a.units[t.unit];
   const BlockDev& B = a.blocks[un.block];
   const int nx = B.sz[0], ny = B.sz[1], nz = B.sz[2];
-  const int I0 = nx - 6, I1 = ny - 6;
   const int i0 = 3 + t.i0, j0 = 3 + t.j0, k0 = 3 + un.k0;
   const int ex = t.ex, ey = t.ey, ez = un.nz;
   const int ox = i0 - kHalo, oy = j0 - kHalo;  // plane origin (padded coords)
@@ -416,8 +422,8 @@ __device__ __forceinline__ void derive_tile(const DerivArgs& a, const TileDev t,
   const bool active = tx < ex && ty < ey;
   const int gi = i0 + tx, gj = j0 + ty;
   // chunk-relative scratch offsets fit in 32 bits (NS * cap < 2^31)
-  const int plane_pts = I0 * I1;
-  const int lp_col = (int)un.sbase + (gi - 3) + I0 * (gj - 3);  // + plane_pts * (z - k0)
+  const int plane_pts = sm.plane_pts;
+  const int lp_col = sm.col_base + tx + sm.row_stride * ty;  // + plane_pts * (z - k0)
   // z reach of the item's rows: closure rows reach 4 planes, centred rows 3
   constexpr int H = CL ? kHalo : 3;
   constexpr int QD = 2 * H + 1;
@@ -593,15 +599,29 @@ __device__ __forceinline__ void derive_tile(const DerivArgs& a, const TileDev t,
   cp_async_wait<0>();
 }
 
+// Two-pass path: item (tile t of a unit, variable v) with the unit's compact scratch
+// numbering.
+template <typename ST, bool DD, bool ADV = false, bool CL = true>
+__device__ __forceinline__ void derive_tile(const DerivArgs& a, const TileDev t, const int v,
+                                            double (*s_plane)[kPlane], void* s_dxp_raw,
+                                            double* s_kq, LineScales* s_sc) {
+  const UnitDev un = a.units[t.unit];
+  const int I0 = a.blocks[un.block].sz[0] - 6, I1 = a.blocks[un.block].sz[1] - 6;
+  const ScratchMap sm{(int)un.sbase + t.i0 + I0 * t.j0, I0, I0 * I1};
+  derive_item<ST, DD, ADV, CL>(a, un, t, sm, v, s_plane, s_dxp_raw, s_kq, s_sc);
+}
+
 // True when some output point of the item lies within three points of a flagged
 // face (closure_row on the tile's x and y ranges or the slab's z range).
-__device__ __forceinline__ bool tile_has_closure(const DerivArgs& a, const TileDev& t) {
-  const UnitDev un = a.units[t.unit];
-  const BlockDev& B = a.blocks[un.block];
+__device__ __forceinline__ bool item_has_closure(const BlockDev& B, const UnitDev& un, const TileDev& t) {
   const uint32_t bf = B.bflag;
   auto near = [](int p0, int e, int n, bool lo, bool hi) { return (lo && p0 < 6) || (hi && p0 + e - 1 >= n - 6); };
   return near(3 + t.i0, t.ex, B.sz[0], bf & 1u, bf & 2u) || near(3 + t.j0, t.ey, B.sz[1], bf & 4u, bf & 8u) ||
          near(3 + un.k0, un.nz, B.sz[2], bf & 16u, bf & 32u);
+}
+__device__ __forceinline__ bool tile_has_closure(const DerivArgs& a, const TileDev& t) {
+  const UnitDev un = a.units[t.unit];
+  return item_has_closure(a.blocks[un.block], un, t);
 }
 
 // Persistent derivative kernel: the grid holds as many CTAs as fit on the GPU at
@@ -801,16 +821,12 @@ __device__ __forceinline__ void prefetch_l2_bulk(const void* p, uint32_t bytes) 
   asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
 }
 
-// The right-hand side of one interior point: local index lpu of unit `un`, inputs
-// through `src`.
+// The right-hand side of interior point (i, j, k) (padded coordinates) of block B,
+// inputs through `src`.
 template <typename RT, int MODE, class Src, bool ADV = false>
-__device__ __forceinline__ void algebra_point(const AlgebraArgs& a, const UnitDev& un, int lpu,
-                                              const Src& src) {
-  const BlockDev& B = a.blocks[un.block];
+__device__ __forceinline__ void algebra_point_at(const AlgebraArgs& a, const BlockDev& B, int i, int j,
+                                                 int k, const Src& src) {
   const int nx = B.sz[0], ny = B.sz[1];
-  const int I0 = nx - 6, I1 = ny - 6;
-  const int lx = lpu % I0, rr = lpu / I0, ly = rr % I1, lz = rr / I1;
-  const int i = lx + 3, j = ly + 3, k = lz + 3 + un.k0;
   const int64_t pp = B.offset + i + (int64_t)nx * (j + (int64_t)ny * k);
   // coordinates as bssnrhs forms them (pmin + i*h, two roundings, rhs.cpp:207-213)
   const double x = __dadd_rn(B.pmin[0], __dmul_rn((double)i, B.h[0]));
@@ -856,6 +872,16 @@ __device__ __forceinline__ void algebra_point(const AlgebraArgs& a, const UnitDe
     bssn_rhs_algebra_adv<RT>(in, sink, *prm, (RT)eta);
   else
     bssn_rhs_algebra<RT>(in, sink, *prm, (RT)eta);
+}
+
+// The same for interior point lpu (compact numbering) of unit `un`.
+template <typename RT, int MODE, class Src, bool ADV = false>
+__device__ __forceinline__ void algebra_point(const AlgebraArgs& a, const UnitDev& un, int lpu,
+                                              const Src& src) {
+  const BlockDev& B = a.blocks[un.block];
+  const int I0 = B.sz[0] - 6, I1 = B.sz[1] - 6;
+  const int lx = lpu % I0, rr = lpu / I0, ly = rr % I1, lz = rr / I1;
+  algebra_point_at<RT, MODE, Src, ADV>(a, B, lx + 3, ly + 3, lz + 3 + un.k0, src);
 }
 
 // One CTA per range of up to 128 consecutive points of a unit, one thread per point,

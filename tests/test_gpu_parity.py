@@ -2,7 +2,7 @@
 the reference's bssnrhs) and the reference's own outputs (golden fixtures).
 
 FP64 bar: per variable, max|gpu - ref| / max|ref| <= 1e-12 over the interior.
-MIXED bar (FP32 algebra): the same norm-wise error <= 1e-5 per variable.
+MIXED bar (FP32 algebra): the same norm-wise error <= 1e-6 per variable (the benchmark's bar).
 """
 import os
 
@@ -16,7 +16,7 @@ from sympygr_b200 import workloads as wl
 pytestmark = pytest.mark.gpu
 
 TOL64 = 1e-12
-TOL_MIXED = 1e-5
+TOL_MIXED = 1e-6
 
 
 def _gpu_block(ctx, u, blk, sigma, precision=sg.FP64, sentinel=np.nan):

@@ -3,7 +3,8 @@ the 4th-order upwind derivatives deriv42adv_* (bssn/src/derivs.cpp:495-900) inst
 the centred 6th-order ones.  Against the oracle's upwind-mode RHS (its upwind operator
 is pinned bit for bit to the reference's deriv42adv_* in the CPU tests).
 
-FP64 bar: per variable, max|gpu - oracle| / max|oracle| <= 1e-12; MIXED <= 1e-5.
+FP64 bar: per variable, max|gpu - oracle| / max|oracle| <= 1e-12 on every block.  MIXED
+bar: the same norm over the batch's blocks <= 1e-6, and <= 1e-5 on every block.
 """
 import numpy as np
 import pytest
@@ -14,7 +15,8 @@ from oracle import pyoracle as po
 pytestmark = pytest.mark.gpu
 
 TOL64 = 1e-12
-TOL_MIXED = 1e-5
+TOL_MIXED = 1e-6
+TOL_MIXED_BLOCK = 1e-5
 SIGMA = 0.25
 
 
@@ -49,11 +51,12 @@ def test_upwind_fp64_vs_oracle(ctx, oracle_lib, chunk_points):
 def test_upwind_mixed_vs_oracle(ctx, oracle_lib):
     u, blocks, total = _batch(seed=3)
     got = _gpu_rhs(ctx, u, blocks, sg.MIXED, True)
-    for b in blocks:
-        ref = po.interior(po.oracle_rhs_adv(u, b, po.params(ko_sigma=SIGMA)), b)
-        mx, _ = po.rel_errors(po.interior(got, b), ref)
-        nz = np.abs(ref).max(axis=1) > 0
-        assert mx[nz].max() < TOL_MIXED, (b, mx.max())
+    pairs = [(po.interior(got, b), po.interior(po.oracle_rhs_adv(u, b, po.params(ko_sigma=SIGMA)), b))
+             for b in blocks]
+    over, per_block = po.batch_rel_errors(pairs)
+    assert over.max() < TOL_MIXED, over
+    for b, e in zip(blocks, per_block):
+        assert e.max() < TOL_MIXED_BLOCK, (b, e.max())
 
 
 def test_upwind_differs_from_centred_only_through_the_shift(ctx):

@@ -381,10 +381,11 @@ def profile_case(args):
     u, blocks = wl.two_puncture_batch_torch((69, 135), (4, 1), seed=5, device="cuda")
     rhs = torch.zeros_like(u)
     ctx = sg.Context(0)
-    plan = sg.Plan(ctx, blocks, prec)
+    plan = sg.Plan(ctx, blocks, prec, single_pass=args.single_pass, ring_slots=args.ring_slots)
     prm = sg.Params.make(ko_sigma=SIGMA, precision=prec)
     for _ in range(2):
         plan.rhs_device(list(rhs), list(u), prm)
+    plan.status()
     if args.profile_steps:
         norms = torch.zeros(len(blocks) * 8, dtype=torch.float64, device="cuda")
         plan.constraints_device(list(u), None, norms)
@@ -395,7 +396,8 @@ def profile_case(args):
         torch.cuda.synchronize()
         rk.close()
     torch.cuda.synchronize()
-    print(json.dumps({"profile_case": args.profile_case, "points": plan.points, "launches": plan.launches}))
+    print(json.dumps({"profile_case": args.profile_case, "single_pass": plan.single_pass, "points": plan.points,
+                      "launches": plan.launches}))
     plan.close()
     ctx.close()
 

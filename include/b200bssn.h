@@ -136,6 +136,15 @@ typedef struct b200bssn_plan_options {
   uint32_t single_pass;
   /* Ring slots of the one-pass kernel (0: 32; each slot 3072 points, 2 MB). */
   uint32_t ring_slots;
+  /* Tile height of the two-pass derivative kernels: 16 x tile_y columns per CTA, one
+   * thread per column (0: 8; also 4 or 16). */
+  uint32_t tile_y;
+  /* Registers-per-thread split of the two-pass derivative kernels (the kinds without /
+   * with second derivatives): 1 = 96 / 128 registers, 2 = 80 / 96 (one CTA per SM
+   * more), 3 = 128 / 168 (one fewer); 2 and 3 with 16x8 tiles and centred advection
+   * only.  0: the measured best -- 3 for FP64 with centred advection and 16x8 tiles,
+   * else 1. */
+  uint32_t deriv_regs;
 } b200bssn_plan_options;
 
 /* b200bssn_plan_create with explicit options (opts may be NULL). */

@@ -6,17 +6,22 @@ class's block count from the batch, times --scale) it builds a plan of that clas
 alone and times one evaluation (CUDA events, device-resident inputs larger than L2)
 for every candidate of
 
-* slab depth: the z-planes per work unit of the derivative kernel (candidates that
-  cut the interior into the same number of slabs are the same plan, so one per
-  slab count is timed);
-* derivative CTAs per SM: as many as fit (0; the kernel over the first-derivative-only
-  variables fits 3, the other 2) or a cap of 1 or 2 on both derivative kernels.
+* tile shape: 16 x tile_y columns per derivative CTA, tile_y 4, 8 or 16 (64, 128 or
+  256 threads; the staged plane, the D_x halo rows and the register queues follow);
+* registers-per-thread split of the derivative kernels: 96 / 128 registers for the kinds
+  without / with second derivatives, one CTA per SM more (80 / 96) or one fewer
+  (128 / 168) -- with 16x8 tiles (the plans' default is the last for FP64, the first
+  for MIXED);
+* slab depth (staging depth along z): the z-planes per work unit of the derivative
+  kernel (candidates that cut the interior into the same number of slabs are the same
+  plan, so one per slab count is timed);
+* with --ctas, derivative CTAs per SM capped at 1 or 2 as well as uncapped.
 
-It writes the per-class table and choice to JSON.  ``tuned_plan`` builds a plan
-for any block list from such a table: each block gets its class's slab depth
-(b200bssn_plan_options.block_slab_depth); the CTA count, a plan-wide knob, is the
-choice of the class holding the most points.  The run ends with the whole batch
-timed with the default knobs and with the tuned ones.
+It writes the per-class table and choice to JSON.  ``tuned_plan`` builds a plan for
+any block list from such a table: each block gets its class's slab depth
+(b200bssn_plan_options.block_slab_depth); the tile shape, register split and CTA
+count, plan-wide knobs, are the choice of the class holding the most points.  The run
+ends with the whole batch timed with the default knobs and with the tuned ones.
 
     python -m sympygr_b200.autotune --precision mixed --json tune_mixed.json
 """
@@ -58,12 +63,20 @@ def time_plan(plan, rhs, u, prm, reps: int = 5, warmup: int = 2) -> float:
     return e0.elapsed_time(e1) / reps
 
 
+# (tile_y, deriv_regs) variants of the derivative kernels built into the library
+# (deriv_regs 1: 96/128 registers for the kinds without/with second derivatives, 2: 80/96,
+# 3: 128/168)
+KERNEL_VARIANTS = [(8, 1), (4, 1), (16, 1), (8, 2), (8, 3)]
+
+
 def tuned_plan(ctx, blocks, precision, table, chunk_points: int = 0):
-    """A plan whose blocks use their size class's tuned slab depth."""
+    """A plan whose blocks use their size class's tuned slab depth and the plan-wide
+    knobs of the class holding the most points."""
     choice = {int(k): v for k, v in table["choice"].items()}
     depths = [choice.get(b.sz[2], {}).get("slab_depth", 0) for b in blocks]
     return capi.Plan(ctx, blocks, precision, chunk_points, deriv_ctas_per_sm=table["deriv_ctas_per_sm"],
-                     block_slab_depth=depths)
+                     block_slab_depth=depths, tile_y=table.get("tile_y", 0),
+                     deriv_regs=table.get("deriv_regs", 0))
 
 
 def main(argv=None):
@@ -74,36 +87,44 @@ def main(argv=None):
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--reps", type=int, default=5)
     ap.add_argument("--json", default="")
+    ap.add_argument("--ctas", action="store_true", help="also sweep CTA caps of 1 and 2 per SM")
     args = ap.parse_args(argv)
     prec = capi.MIXED if args.precision == "mixed" else capi.FP64
     prm = capi.Params.make(ko_sigma=0.4, precision=prec)
     ctx = capi.Context(0)
     counts = tuple(max(1, int(round(c * args.scale))) for c in wl.BATCH_COUNTS)
     table = {"precision": args.precision, "classes": {}, "choice": {}}
-    best_points = (0, 0)
+    best_points = (0, None)
     for n, c in zip(wl.BATCH_SIZES, counts):
         u, blocks = wl.two_puncture_batch_torch((n,), (c,), seed=1, device="cuda")
         rhs = torch.zeros_like(u)
         pts = sum(b.ninterior for b in blocks)
         rows = []
-        for d in depth_candidates(n):
-            for ctas in (0, 1, 2):
-                plan = capi.Plan(ctx, blocks, prec, slab_depth=d, deriv_ctas_per_sm=ctas)
-                ms = time_plan(plan, list(rhs), list(u), prm, args.reps)
-                plan.close()
-                rows.append({"slab_depth": d, "deriv_ctas_per_sm": ctas, "ms": ms,
-                             "mpts_per_s": pts / ms / 1e3})
-                print(json.dumps({"class": n, **rows[-1]}), flush=True)
+        for ty, regs in KERNEL_VARIANTS:
+            for d in depth_candidates(n):
+                for ctas in ((0, 1, 2) if args.ctas else (0,)):
+                    plan = capi.Plan(ctx, blocks, prec, slab_depth=d, deriv_ctas_per_sm=ctas, tile_y=ty,
+                                     deriv_regs=regs)
+                    ms = time_plan(plan, list(rhs), list(u), prm, args.reps)
+                    plan.close()
+                    rows.append({"tile_y": ty, "deriv_regs": regs, "slab_depth": d, "deriv_ctas_per_sm": ctas,
+                                 "ms": ms, "mpts_per_s": pts / ms / 1e3})
+                    print(json.dumps({"class": n, **rows[-1]}), flush=True)
         best = max(rows, key=lambda r: r["mpts_per_s"])
+        nslab = lambda d: -(-(n - 6) // d)  # noqa: E731 -- slabs of the class's blocks at depth d
+        dregs = 3 if prec == capi.FP64 else 1  # the plan's default split for this precision
+        default = next(r for r in rows if r["tile_y"] == 8 and r["deriv_regs"] == dregs and r["deriv_ctas_per_sm"] == 0
+                       and nslab(r["slab_depth"]) == nslab(48))
         table["classes"][str(n)] = {"blocks": c, "points": pts, "runs": rows}
-        table["choice"][str(n)] = {"slab_depth": best["slab_depth"],
-                                   "deriv_ctas_per_sm": best["deriv_ctas_per_sm"],
-                                   "mpts_per_s": best["mpts_per_s"]}
+        table["choice"][str(n)] = {k: best[k] for k in ("tile_y", "deriv_regs", "slab_depth", "deriv_ctas_per_sm",
+                                                        "mpts_per_s")}
+        table["choice"][str(n)]["gain_over_default"] = best["mpts_per_s"] / default["mpts_per_s"]
         if pts > best_points[0]:
-            best_points = (pts, best["deriv_ctas_per_sm"])
+            best_points = (pts, best)
         del u, rhs
         torch.cuda.empty_cache()
-    table["deriv_ctas_per_sm"] = best_points[1]
+    for k in ("deriv_ctas_per_sm", "tile_y", "deriv_regs"):
+        table[k] = best_points[1][k]
     # the whole batch: default knobs against the tuned table
     u, blocks = wl.two_puncture_batch_torch(wl.BATCH_SIZES, counts, seed=0, device="cuda")
     rhs = torch.zeros_like(u)
@@ -117,7 +138,8 @@ def main(argv=None):
     table["batch"] = {"points": pts, "default_mpts_per_s": pts / ms_default / 1e3,
                       "tuned_mpts_per_s": pts / ms_tuned / 1e3}
     print(json.dumps({"choice": table["choice"], "batch": table["batch"],
-                      "deriv_ctas_per_sm": table["deriv_ctas_per_sm"]}), flush=True)
+                      "plan_wide": {k: table[k] for k in ("deriv_ctas_per_sm", "tile_y", "deriv_regs")}}),
+          flush=True)
     if args.json:
         with open(args.json, "w") as f:
             json.dump(table, f, indent=1)

@@ -64,12 +64,39 @@ void make_args(const b200bssn_plan* P, double* const* rhs, const double* const* 
   aa.ko_sigma = prm->ko_sigma;
 }
 
+// The derivative kind kernels built for each plan knob: tile height 4, 8 or 16 with the
+// default register split, and 16x8 tiles with one CTA per SM more or fewer (the upwind
+// mode only with the defaults).  Returns the kernel, or nullptr if not built.
+template <typename ST, bool ADV, int TY, int REGV>
+const void* kind_ptr(bool dd) {
+  return dd ? (const void*)bssn_derivs_kind_kernel<ST, true, ADV, TY, REGV>
+            : (const void*)bssn_derivs_kind_kernel<ST, false, ADV, TY, REGV>;
+}
+const void* kind_kernel(bool mixed, bool adv, bool dd, int ty, int regv) {
+  if (adv) {
+    if (ty != kTileY || regv != 0) return nullptr;
+    return mixed ? kind_ptr<float, true, kTileY, 0>(dd) : kind_ptr<double, true, kTileY, 0>(dd);
+  }
+#define B200BSSN_KIND(TYV, RV) \
+  if (ty == TYV && regv == RV) return mixed ? kind_ptr<float, false, TYV, RV>(dd) : kind_ptr<double, false, TYV, RV>(dd);
+  B200BSSN_KIND(8, 0)
+  B200BSSN_KIND(8, 1)
+  B200BSSN_KIND(8, 2)
+  B200BSSN_KIND(4, 0)
+  B200BSSN_KIND(16, 0)
+#undef B200BSSN_KIND
+  return nullptr;
+}
+
 // The derivative stage of one chunk: the kernels over the variables without and with
 // second derivatives, each with its own work counter.
-template <typename ST, bool ADV>
-void launch_derivs(const DerivArgs& dn, const DerivArgs& dd, int gn, int gd, cudaStream_t s) {
-  bssn_derivs_kind_kernel<ST, false, ADV><<<gn, kDerivThreads, 0, s>>>(dn);
-  bssn_derivs_kind_kernel<ST, true, ADV><<<gd, kDerivThreads, 0, s>>>(dd);
+int launch_derivs(b200bssn_plan* P, DerivArgs dn, DerivArgs dd, int gn, int gd, cudaStream_t s) {
+  void* an[] = {&dn};
+  void* ad[] = {&dd};
+  const dim3 block((unsigned)(kTileX * P->tile_y));
+  CK(P->ctx, cudaLaunchKernel(P->kind_fn[0], dim3((unsigned)gn), block, an, 0, s));
+  CK(P->ctx, cudaLaunchKernel(P->kind_fn[1], dim3((unsigned)gd), block, ad, 0, s));
+  return B200BSSN_OK;
 }
 
 // The staged algebra kernel for the RK mode of `aa` (RK_NONE: store the RHS).
@@ -132,12 +159,8 @@ int enqueue_chunk(b200bssn_plan* P, DerivArgs da, AlgebraArgs aa, size_t ci, int
     dd.counter = P->d_counters + 2 * ci + 1;
     const int gn = std::min(c.tile_count * kKindVars[0], P->deriv_grid[0]);
     const int gd = std::min(c.tile_count * kKindVars[1], P->deriv_grid[1]);
-    if (mixed)
-      P->advective ? launch_derivs<float, true>(dn, dd, gn, gd, s1)
-                   : launch_derivs<float, false>(dn, dd, gn, gd, s1);
-    else
-      P->advective ? launch_derivs<double, true>(dn, dd, gn, gd, s1)
-                   : launch_derivs<double, false>(dn, dd, gn, gd, s1);
+    const int rc = launch_derivs(P, dn, dd, gn, gd, s1);
+    if (rc != B200BSSN_OK) return rc;
   }
   CK(ctx, cudaGetLastError());
   if (ev) CK(ctx, cudaEventRecord(ev[4 * ci + 1], s1));
@@ -184,9 +207,7 @@ int launch_single_pass(b200bssn_plan* P, const DerivArgs& da, const AlgebraArgs&
   f.d.koscr = P->fring_k;
   f.d.cap = P->nring * kFusedSlotPts;
   f.tiles = P->d_ftiles;
-  f.group_tile = P->d_group_tile;
   f.ntiles = (int32_t)P->ftiles.size();
-  f.ngroups = P->ngroups;
   f.nring = P->nring;
   f.sync = P->d_fsync;
   CK(ctx, cudaMemsetAsync(P->d_fsync, 0, P->fsync_words * sizeof(int), s));
@@ -386,6 +407,19 @@ int b200bssn_plan_create_ex(b200bssn_ctx* ctx, const b200bssn_block* blocks, uin
   P->ctx = ctx;
   P->precision = precision;
   P->advective = o.advective != 0;
+  P->tile_y = o.tile_y ? (int)o.tile_y : kTileY;
+  // register split: option 1 = 96/128 registers (the kinds without / with second
+  // derivatives), 2 = 80/96, 3 = 128/168; 0 = the measured best for the precision
+  // (FP64 with centred advection: 128/168, 4 % faster on the batch; else 96/128)
+  const uint32_t regs_opt = o.deriv_regs ? o.deriv_regs
+                                         : (precision == B200BSSN_FP64 && !P->advective && P->tile_y == kTileY ? 3u : 1u);
+  P->deriv_regs = regs_opt >= 1 && regs_opt <= 3 ? (int)regs_opt - 1 : -1;  // kernel variant
+  for (int k = 0; k < 2; ++k)
+    P->kind_fn[k] = kind_kernel(precision == B200BSSN_MIXED, P->advective, k == 1, P->tile_y, P->deriv_regs);
+  if (!P->kind_fn[0] || !P->kind_fn[1]) {
+    delete P;
+    return B200BSSN_ERR_INVALID_ARGUMENT;
+  }
   const int nslots = P->advective ? kNumDerivs + 3 * kNumVars : kNumDerivs;
   const int64_t kMaxChunkPoints = max_chunk_points(nslots);
   P->span_lo = UINT64_MAX;
@@ -471,14 +505,14 @@ int b200bssn_plan_create_ex(b200bssn_ctx* ctx, const b200bssn_block* blocks, uin
     cur.points = (cur.points + 31) & ~int64_t(31);  // slot runs start 128-byte aligned
     u.sbase = cur.points;
     cur.points += np;
-    for (int j0 = 0; j0 < I1; j0 += kTileY)
+    for (int j0 = 0; j0 < I1; j0 += P->tile_y)
       for (int i0 = 0; i0 < I0; i0 += kTileX) {
         TileDev t;
         t.unit = (int32_t)ui;
         t.i0 = (int16_t)i0;
         t.j0 = (int16_t)j0;
         t.ex = (int16_t)std::min(kTileX, I0 - i0);
-        t.ey = (int16_t)std::min(kTileY, I1 - j0);
+        t.ey = (int16_t)std::min(P->tile_y, I1 - j0);
         P->tiles.push_back(t);
       }
     for (int64_t s = 0; s < np; s += kAlgebraThreads) {
@@ -529,18 +563,9 @@ int b200bssn_plan_create_ex(b200bssn_ctx* ctx, const b200bssn_block* blocks, uin
     int sms = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
     const bool mx = precision == B200BSSN_MIXED, adv = P->advective;
-    const void* kinds[2] = {
-        mx ? (adv ? (const void*)bssn_derivs_kind_kernel<float, false, true>
-                  : (const void*)bssn_derivs_kind_kernel<float, false, false>)
-           : (adv ? (const void*)bssn_derivs_kind_kernel<double, false, true>
-                  : (const void*)bssn_derivs_kind_kernel<double, false, false>),
-        mx ? (adv ? (const void*)bssn_derivs_kind_kernel<float, true, true>
-                  : (const void*)bssn_derivs_kind_kernel<float, true, false>)
-           : (adv ? (const void*)bssn_derivs_kind_kernel<double, true, true>
-                  : (const void*)bssn_derivs_kind_kernel<double, true, false>)};
     for (int k = 0; k < 2; ++k) {
       int per_sm = 0;
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kinds[k], kDerivThreads, 0);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, P->kind_fn[k], kTileX * P->tile_y, 0);
       if (o.deriv_ctas_per_sm) per_sm = std::min<int>(per_sm, (int)o.deriv_ctas_per_sm);
       P->deriv_grid[k] = std::max(1, sms * std::max(1, per_sm));
     }
@@ -601,10 +626,7 @@ int b200bssn_plan_create_ex(b200bssn_ctx* ctx, const b200bssn_block* blocks, uin
       return B200BSSN_ERR_SIZE_LIMIT;
     }
     P->ngroups = (int32_t)groups;
-    P->group_tile.resize((size_t)groups);
-    for (size_t t = 0; t < P->ftiles.size(); ++t)
-      for (int z = 0; z < P->ftiles[t].nz; ++z) P->group_tile[(size_t)P->ftiles[t].group_base + z] = (int32_t)t;
-    P->fsync_words = 4 + 2 * P->ftiles.size() + (size_t)P->nring;
+    P->fsync_words = 4 + 3 * P->ftiles.size() + (size_t)P->nring;
     int sms = 0, per_sm = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bssn_fused_kernel<RK_NONE>, kFusedThreads,
@@ -626,19 +648,15 @@ int b200bssn_plan_create_ex(b200bssn_ctx* ctx, const b200bssn_block* blocks, uin
     if (e == cudaSuccess) e = cudaMalloc(&P->koscr[b], (size_t)kNumVars * P->cap * st + 512);
   }
   if (e == cudaSuccess && P->single_pass) {
-    const size_t ntb = al(P->ftiles.size() * sizeof(FusedTileDev)), ngb = al(P->group_tile.size() * sizeof(int32_t));
-    e = cudaMalloc(&P->fdesc, ntb + ngb + al(P->fsync_words * sizeof(int)));
+    const size_t ntb = al(P->ftiles.size() * sizeof(FusedTileDev));
+    e = cudaMalloc(&P->fdesc, ntb + al(P->fsync_words * sizeof(int)));
     if (e == cudaSuccess) {
       char* fb = static_cast<char*>(P->fdesc);
       P->d_ftiles = reinterpret_cast<FusedTileDev*>(fb);
-      P->d_group_tile = reinterpret_cast<int32_t*>(fb + ntb);
-      P->d_fsync = reinterpret_cast<int*>(fb + ntb + ngb);
+      P->d_fsync = reinterpret_cast<int*>(fb + ntb);
       e = cudaMemcpy(P->d_ftiles, P->ftiles.data(), P->ftiles.size() * sizeof(FusedTileDev),
                      cudaMemcpyHostToDevice);
     }
-    if (e == cudaSuccess)
-      e = cudaMemcpy(P->d_group_tile, P->group_tile.data(), P->group_tile.size() * sizeof(int32_t),
-                     cudaMemcpyHostToDevice);
     const size_t ring_pts = (size_t)P->nring * kFusedSlotPts;
     if (e == cudaSuccess) e = cudaMalloc(&P->fring_d, ring_pts * kNumDerivs * sizeof(float) + 512);
     if (e == cudaSuccess) e = cudaMalloc(&P->fring_k, ring_pts * kNumVars * sizeof(float) + 512);

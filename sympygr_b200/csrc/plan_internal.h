@@ -73,17 +73,18 @@ struct b200bssn_plan {
   bool host_pipeline = false;
   std::vector<uint64_t> part;
   std::vector<cudaEvent_t> ev_in;  // per chunk: upload done
+  int tile_y = b200bssn::kTileY;      // tile height of the derivative kernels (4, 8 or 16)
+  int deriv_regs = 0;                 // register split variant of the derivative kernels
+  const void* kind_fn[2] = {nullptr, nullptr};  // the derivative kind kernels (without / with DD)
   int deriv_grid[2] = {0, 0};  // resident CTAs of the two persistent derivative kernels
   int alg_grid = 0;           // resident CTAs of the persistent staged algebra kernel (MIXED)
-  // one-pass path (MIXED, centred advection): tile-slabs in launch order, the tile-slab
-  // of every algebra group, the per-evaluation sync words and the scratch ring
+  // one-pass path (MIXED, centred advection): tile-slabs in launch order, the
+  // per-evaluation sync words and the scratch ring
   bool single_pass = false;
   int32_t nring = 0, ngroups = 0, fused_grid = 0;
   std::vector<b200bssn::FusedTileDev> ftiles;
-  std::vector<int32_t> group_tile;
   void* fdesc = nullptr;
   b200bssn::FusedTileDev* d_ftiles = nullptr;
-  int32_t* d_group_tile = nullptr;
   int* d_fsync = nullptr;
   size_t fsync_words = 0;
   void* fring_d = nullptr;  // nring * kFusedSlotPts points x 138 slots (float)

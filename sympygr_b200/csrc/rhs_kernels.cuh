@@ -85,6 +85,20 @@ constexpr int kStageRows = kPlaneH / (kDerivThreads / 32);
 static_assert(kStageRows * (kDerivThreads / 32) == kPlaneH, "plane rows split evenly over the warps");
 static_assert(kDxRows <= 2 * kTileY, "two D_x halo rows per thread cover the plane");
 
+// Shape of a derivative CTA for tiles of 16 x TY columns (TY = 4, 8 or 16): one thread
+// per column, the staged plane with its 4-point halo, the y-halo D_x rows.
+template <int TY>
+struct TileShape {
+  static constexpr int kThreads = kTileX * TY;
+  static constexpr int kWarps = kThreads / 32;
+  static constexpr int kPlaneH = TY + 2 * kHalo;
+  static constexpr int kPlane = kPlaneW * kPlaneH;
+  static constexpr int kDxRows = TY + 2 * kHalo;
+  static constexpr int kDxPerThread = (kDxRows + TY - 1) / TY;  // D_x halo rows per thread
+  static constexpr int kStageRows = kPlaneH / kWarps;           // plane rows per thread
+  static_assert(kStageRows * kWarps == kPlaneH, "plane rows split evenly over the warps");
+};
+
 // the copy is issued only when `p` holds; otherwise nothing is read or written
 __device__ __forceinline__ void cp_async8_if(double* smem_dst, const double* gmem_src, bool p) {
   const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
@@ -242,10 +256,10 @@ __device__ __forceinline__ void q_push(T (&q)[N], T v) {
 // only through FP64 differences taken before any downcast -- antisymmetric
 // a_k = u(+k) - u(-k) for first derivatives, symmetric s_k = u(+k) + u(-k) - 2u
 // for second derivatives (the centre weight cancels exactly since the weights
-// sum to zero) -- and the weighted sum of the rounded differences runs in FP32,
-// the precision the derivative is stored in.  The Kreiss-Oliger row, a sixth
-// difference that cancels all lower orders, stays in FP64 (from the same
-// symmetric sums, fused multiply-adds allowed).
+// sum to zero) -- whose weighted sum (fused multiply-adds allowed) is rounded once
+// to FP32, the precision the derivative is stored in.  The Kreiss-Oliger row, a
+// sixth difference that cancels all lower orders, stays in FP64 (from the same
+// symmetric sums).
 struct ExactRows {
   using D = double;
   template <typename T, int N>
@@ -293,12 +307,14 @@ struct ExactRows {
 
 struct SplitRows {
   using D = float;
+  // the weighted sum of the FP64 differences is formed in FP64 and rounded once to the
+  // FP32 of the slot: one rounding instead of four, and no conversion per difference
   template <typename T, int N>
   static __device__ __forceinline__ D d1(const T (&w)[N], int C, const LineScales& c) {
-    const float a1 = (float)(w[C + 1] - w[C - 1]);
-    const float a2 = (float)(w[C + 2] - w[C - 2]);
-    const float a3 = (float)(w[C + 3] - w[C - 3]);
-    return fmaf(45.0f, a1, fmaf(-9.0f, a2, a3)) * (float)c.d1_c;
+    const double a1 = (double)w[C + 1] - (double)w[C - 1];
+    const double a2 = (double)w[C + 2] - (double)w[C - 2];
+    const double a3 = (double)w[C + 3] - (double)w[C - 3];
+    return (float)(fma(45.0, a1, fma(-9.0, a2, a3)) * c.d1_c);
   }
   // D_x / D_y fields that feed the mixed derivatives stay FP64: differencing
   // FP32-rounded first derivatives would cancel their leading digits
@@ -312,10 +328,10 @@ struct SplitRows {
   template <int N>
   static __device__ __forceinline__ D d2(const double (&w)[N], int C, const LineScales& c) {
     const double u2 = 2.0 * w[C];
-    const float s1 = (float)((w[C + 1] + w[C - 1]) - u2);
-    const float s2 = (float)((w[C + 2] + w[C - 2]) - u2);
-    const float s3 = (float)((w[C + 3] + w[C - 3]) - u2);
-    return fmaf(270.0f, s1, fmaf(-27.0f, s2, 2.0f * s3)) * (float)c.d2_c;
+    const double s1 = (w[C + 1] + w[C - 1]) - u2;
+    const double s2 = (w[C + 2] + w[C - 2]) - u2;
+    const double s3 = (w[C + 3] + w[C - 3]) - u2;
+    return (float)(fma(270.0, s1, fma(-27.0, s2, 2.0 * s3)) * c.d2_c);
   }
   template <int N>
   static __device__ __forceinline__ double ko(const double (&w)[N], int C, const LineScales& c) {
@@ -399,11 +415,12 @@ struct ScratchMap {
   int32_t col_base, row_stride, plane_pts;
 };
 
-template <typename ST, bool DD, bool ADV = false, bool CL = true>
+template <typename ST, bool DD, bool ADV = false, bool CL = true, int TY = kTileY>
 __device__ __forceinline__ void derive_item(const DerivArgs& a, const UnitDev& un, const TileDev& t,
-                                            const ScratchMap sm, const int v, double (*s_plane)[kPlane],
+                                            const ScratchMap sm, const int v, double* s_plane,
                                             void* s_dxp_raw, double* s_kq, LineScales* s_sc) {
   using Rows = typename RowsFor<ST>::type;
+  using SH = TileShape<TY>;
   constexpr int NS = ADV ? kNumDerivs + 3 * kNumVars : kNumDerivs;  // slots per point
   double* s_dxp = static_cast<double*>(s_dxp_raw);
   const BlockDev& B = a.blocks[un.block];
@@ -436,24 +453,24 @@ __device__ __forceinline__ void derive_item(const DerivArgs& a, const UnitDev& u
   // the 32-wide staging grid (24 columns used), every (warps per CTA)-th row of the
   // plane from its warp's index on.
   const int sbx = threadIdx.x & 31, sby0 = threadIdx.x >> 5;
-  int st_soff[kStageRows], st_goff[kStageRows];
-  bool st_ok[kStageRows];
+  int st_soff[SH::kStageRows], st_goff[SH::kStageRows];
+  bool st_ok[SH::kStageRows];
 #pragma unroll
-  for (int r = 0; r < kStageRows; ++r) {
-    const int by = sby0 + (kDerivThreads / 32) * r, pi = ox + sbx, pj = oy + by;
+  for (int r = 0; r < SH::kStageRows; ++r) {
+    const int by = sby0 + SH::kWarps * r, pi = ox + sbx, pj = oy + by;
     st_ok[r] = sbx < kPlaneW && pi >= xlo && pi < xhi && pj >= ylo && pj < yhi;
     st_soff[r] = by * kPlaneW + sbx;
     st_goff[r] = pi + nx * pj;
   }
-  // and of the y-halo D_x rows: column dxx, rows dyy0 and dyy0 + kTileY
+  // and of the y-halo D_x rows: column dxx, rows dyy0, dyy0 + TY, ...
   const int dxx = threadIdx.x & 15, dyy0 = threadIdx.x >> 4;
   const int dpi = i0 + dxx;
   const bool dcl = closure_row(dpi, nx, lox, hix);
-  bool dx_ok[2];
+  bool dx_ok[SH::kDxPerThread];
 #pragma unroll
-  for (int r = 0; r < 2; ++r) {
-    const int yy = dyy0 + kTileY * r, pj = oy + yy;
-    dx_ok[r] = yy < kDxRows && dxx < ex && pj >= ylo && pj < yhi;
+  for (int r = 0; r < SH::kDxPerThread; ++r) {
+    const int yy = dyy0 + TY * r, pj = oy + yy;
+    dx_ok[r] = yy < SH::kDxRows && dxx < ex && pj >= ylo && pj < yhi;
   }
   const int64_t plane_elems = (int64_t)nx * ny;
 
@@ -470,7 +487,8 @@ __device__ __forceinline__ void derive_item(const DerivArgs& a, const UnitDev& u
     const double* fp = f + plane_elems * zi;
     const bool in = zi < zload;
 #pragma unroll
-    for (int r = 0; r < kStageRows; ++r) cp_async8_if(&s_plane[b][st_soff[r]], fp + st_goff[r], in && st_ok[r]);
+    for (int r = 0; r < SH::kStageRows; ++r)
+      cp_async8_if(s_plane + b * SH::kPlane + st_soff[r], fp + st_goff[r], in && st_ok[r]);
     cp_async_commit();
   };
 
@@ -484,9 +502,9 @@ __device__ __forceinline__ void derive_item(const DerivArgs& a, const UnitDev& u
   auto dx_rows = [&](int zp, const double* P, double* dst) {
     if (zp < zload) {
 #pragma unroll
-      for (int r = 0; r < 2; ++r) {
+      for (int r = 0; r < SH::kDxPerThread; ++r) {
         if (dx_ok[r]) {
-          const int yy = dyy0 + kTileY * r;
+          const int yy = dyy0 + TY * r;
           const double* p = P + yy * kPlaneW + dxx + kHalo;
           double w[7];
 #pragma unroll
@@ -502,17 +520,17 @@ __device__ __forceinline__ void derive_item(const DerivArgs& a, const UnitDev& u
   if (DD) {
     cp_async_wait<2>();
     __syncthreads();  // plane zs (and the line scales) visible to every thread
-    dx_rows(zs, s_plane[0], s_dxp);
+    dx_rows(zs, s_plane, s_dxp);
   }
   for (int zi = zs, b = 0; zi < zend; ++zi, b = (b + 1) & 3) {
     cp_async_wait<1>();
     __syncthreads();
     stage(zi + 3, (b + 3) & 3);
-    const double* P = s_plane[b];
-    const double* Dxp = s_dxp + ((zi - zs) & 1) * (kDxRows * kTileX);
+    const double* P = s_plane + b * SH::kPlane;
+    const double* Dxp = s_dxp + ((zi - zs) & 1) * (SH::kDxRows * kTileX);
     const bool in_block = zi < nz;
     const bool out_plane = zi >= k0 && zi < k0 + ez;
-    if (DD) dx_rows(zi + 1, s_plane[(b + 1) & 3], s_dxp + ((zi + 1 - zs) & 1) * (kDxRows * kTileX));
+    if (DD) dx_rows(zi + 1, s_plane + ((b + 1) & 3) * SH::kPlane, s_dxp + ((zi + 1 - zs) & 1) * (SH::kDxRows * kTileX));
 
     double dx = 0.0, dy = 0.0, kxy = 0.0, u0 = 0.0;
     if (active && in_block) {
@@ -535,7 +553,7 @@ __device__ __forceinline__ void derive_item(const DerivArgs& a, const UnitDev& u
         const int lp = lp_col + plane_pts * (zi - k0);
         const double kx = clx ? cl_ko(pc, 1, gi, nx, lox, hix, cx) : Rows::ko(wx, 3, cx);
         const double ky = cly ? cl_ko(pc, kPlaneW, gj, ny, loy, hiy, cy) : Rows::ko(wy, 3, cy);
-        s_kq[kslot * kDerivThreads + threadIdx.x] = __dadd_rn(kx, ky);
+        s_kq[kslot * SH::kThreads + threadIdx.x] = __dadd_rn(kx, ky);
         put_slot<NS, ST>(a, 3 * v + 0, lp, dx);
         put_slot<NS, ST>(a, 3 * v + 1, lp, dy);
         if (DD) {
@@ -567,7 +585,7 @@ __device__ __forceinline__ void derive_item(const DerivArgs& a, const UnitDev& u
     }
     // (ko_x + ko_y) of plane zi - H, written H steps ago into slot kslot - H (mod H + 1)
     const int kold = kslot == H ? 0 : kslot + 1;
-    kxy = s_kq[kold * kDerivThreads + threadIdx.x];
+    kxy = s_kq[kold * SH::kThreads + threadIdx.x];
     kslot = kold;
 
     // z derivatives of plane zo = zi - H, whose +-H neighbourhood is now queued
@@ -601,14 +619,14 @@ __device__ __forceinline__ void derive_item(const DerivArgs& a, const UnitDev& u
 
 // Two-pass path: item (tile t of a unit, variable v) with the unit's compact scratch
 // numbering.
-template <typename ST, bool DD, bool ADV = false, bool CL = true>
+template <typename ST, bool DD, bool ADV = false, bool CL = true, int TY = kTileY>
 __device__ __forceinline__ void derive_tile(const DerivArgs& a, const TileDev t, const int v,
-                                            double (*s_plane)[kPlane], void* s_dxp_raw,
+                                            double* s_plane, void* s_dxp_raw,
                                             double* s_kq, LineScales* s_sc) {
   const UnitDev un = a.units[t.unit];
   const int I0 = a.blocks[un.block].sz[0] - 6, I1 = a.blocks[un.block].sz[1] - 6;
   const ScratchMap sm{(int)un.sbase + t.i0 + I0 * t.j0, I0, I0 * I1};
-  derive_item<ST, DD, ADV, CL>(a, un, t, sm, v, s_plane, s_dxp_raw, s_kq, s_sc);
+  derive_item<ST, DD, ADV, CL, TY>(a, un, t, sm, v, s_plane, s_dxp_raw, s_kq, s_sc);
 }
 
 // True when some output point of the item lies within three points of a flagged
@@ -649,14 +667,14 @@ bssn_derivs_kernel(const __grid_constant__ DerivArgs a) {
     const bool cl = tile_has_closure(a, t);
     if (dd_index(v) >= 0) {
       if (cl)
-        derive_tile<ST, true, false, true>(a, t, v, s_plane, s_dxp, s_kq, s_sc);
+        derive_tile<ST, true, false, true>(a, t, v, &s_plane[0][0], s_dxp, s_kq, s_sc);
       else
-        derive_tile<ST, true, false, false>(a, t, v, s_plane, s_dxp, s_kq, s_sc);
+        derive_tile<ST, true, false, false>(a, t, v, &s_plane[0][0], s_dxp, s_kq, s_sc);
     } else {
       if (cl)
-        derive_tile<ST, false, false, true>(a, t, v, s_plane, s_dxp, s_kq, s_sc);
+        derive_tile<ST, false, false, true>(a, t, v, &s_plane[0][0], s_dxp, s_kq, s_sc);
       else
-        derive_tile<ST, false, false, false>(a, t, v, s_plane, s_dxp, s_kq, s_sc);
+        derive_tile<ST, false, false, false>(a, t, v, &s_plane[0][0], s_dxp, s_kq, s_sc);
     }
   }
 }
@@ -678,19 +696,24 @@ __device__ __forceinline__ int kind_var(bool dd, int i) {
   return dd ? kDD[i] : kND[i];
 }
 constexpr int kKindVars[2] = {13, 11};        // [DD]
-// launch-bound occupancy of a kind kernel: the upwind first-derivative kind keeps 6
-// CTAs per SM (80 registers; 5 measured 4 % slower there)
-constexpr int kind_ctas_per_sm(bool dd, bool adv) {
-  return (dd ? 512 : (adv ? 768 : 640)) / kDerivThreads;
+// Launch-bound occupancy of a kind kernel (its registers-per-thread split): the CTAs
+// per SM for 16x8 tiles -- 5 for the first-derivative kind (96 registers; the upwind
+// first-derivative kind keeps 6: 5 measured 4 % slower there), 4 for the second-
+// derivative kind (128) -- scaled to keep the warps per SM for other tile heights;
+// variant REGV 1 asks for one more CTA per SM (fewer registers), 2 for one fewer.
+constexpr int kind_ctas_per_sm(bool dd, bool adv, int ty = kTileY, int regv = 0) {
+  const int base = (dd ? 512 : (adv ? 768 : 640)) / (kTileX * ty);
+  return regv == 1 ? base + 1 : (regv == 2 ? (base > 1 ? base - 1 : 1) : base);
 }
 
-template <typename ST, bool DD, bool ADV = false>
-__global__ void __launch_bounds__(kDerivThreads, kind_ctas_per_sm(DD, ADV))
+template <typename ST, bool DD, bool ADV = false, int TY = kTileY, int REGV = 0>
+__global__ void __launch_bounds__(TileShape<TY>::kThreads, kind_ctas_per_sm(DD, ADV, TY, REGV))
 bssn_derivs_kind_kernel(const __grid_constant__ DerivArgs a) {
+  using SH = TileShape<TY>;
   constexpr int NV = kKindVars[DD];
-  __shared__ double s_plane[4][kPlane];
-  __shared__ double s_dxp[DD ? 2 * kDxRows * kTileX : 1];
-  __shared__ double s_kq[(kHalo + 1) * kDerivThreads];
+  __shared__ double s_plane[4 * SH::kPlane];
+  __shared__ double s_dxp[DD ? 2 * SH::kDxRows * kTileX : 1];
+  __shared__ double s_kq[(kHalo + 1) * SH::kThreads];
   __shared__ LineScales s_sc[3];
   __shared__ int s_item;
   for (;;) {
@@ -701,9 +724,9 @@ bssn_derivs_kind_kernel(const __grid_constant__ DerivArgs a) {
     if (item >= a.tile_count * NV) break;
     const TileDev t = a.tiles[a.tile_base + item / NV];
     if (tile_has_closure(a, t))
-      derive_tile<ST, DD, ADV, true>(a, t, kind_var(DD, item % NV), s_plane, s_dxp, s_kq, s_sc);
+      derive_tile<ST, DD, ADV, true, TY>(a, t, kind_var(DD, item % NV), s_plane, s_dxp, s_kq, s_sc);
     else
-      derive_tile<ST, DD, ADV, false>(a, t, kind_var(DD, item % NV), s_plane, s_dxp, s_kq, s_sc);
+      derive_tile<ST, DD, ADV, false, TY>(a, t, kind_var(DD, item % NV), s_plane, s_dxp, s_kq, s_sc);
   }
 }
 

@@ -4,7 +4,7 @@ the centred 6th-order ones.  Against the oracle's upwind-mode RHS (its upwind op
 is pinned bit for bit to the reference's deriv42adv_* in the CPU tests).
 
 FP64 bar: per variable, max|gpu - oracle| / max|oracle| <= 1e-12 on every block.  MIXED
-bar: the same norm over the batch's blocks <= 1e-6, and <= 1e-5 on every block.
+bar: the same norm over the batch's blocks <= 1e-6, and <= 2e-5 on every block.
 """
 import numpy as np
 import pytest
@@ -16,7 +16,7 @@ pytestmark = pytest.mark.gpu
 
 TOL64 = 1e-12
 TOL_MIXED = 1e-6
-TOL_MIXED_BLOCK = 1e-5
+TOL_MIXED_BLOCK = 2e-5
 SIGMA = 0.25
 
 

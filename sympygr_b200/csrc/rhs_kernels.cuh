@@ -111,11 +111,6 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
-template <int NS, typename ST, typename V>
-__device__ __forceinline__ void put_slot(const DerivArgs& a, int slot, int lp, V val) {
-  static_cast<ST*>(a.dscr)[scr_index<NS>(slot, lp)] = (ST)val;
-}
-
 // Z-direction rows on a queue q[0..8] holding planes zo-4 .. zo+4 of one column.
 // `zc` selects the row: -1 centred, 0..2 the low-side closure rows (zo = 3,4,5),
 // 3..5 the high-side rows (zo = n-6, n-5, n-4); indices are compile-time in every
@@ -476,6 +471,15 @@ __device__ __forceinline__ void derive_item(const DerivArgs& a, const UnitDev& u
 
   const int q = DD ? dd_index(v) : -1;
   const double* __restrict__ f = a.u[v] + B.offset;
+  // The item's scratch columns: slot s of point lp sits at (lp / 32) * 32 NS + s * 32 +
+  // lp % 32 (scr_index), so per output point one offset serves every slot of the
+  // variable, each store adding a constant.
+  ST* const sd_first = static_cast<ST*>(a.dscr) + (3 * v) * 32;                        // D_x, D_y, D_z
+  ST* const sd_second = static_cast<ST*>(a.dscr) + (72 + 6 * (DD ? q : 0)) * 32;       // the 6 second
+  ST* const sd_adv = static_cast<ST*>(a.dscr) + (kNumDerivs + 3 * v) * 32;              // upwind mode
+  ST* const sk = static_cast<ST*>(a.koscr) + v * 32;                                     // KO sum
+  auto col = [](int lp) { return (lp >> 5) * (NS * 32) + (lp & 31); };
+  auto kcol = [](int lp) { return (lp >> 5) * (kNumVars * 32) + (lp & 31); };
   double qu[QD], qx[QD], qy[QD];  // planes zi-2H .. zi of u, D_x u, D_y u (D_x/D_y: DD only)
   int kslot = 0;  // ring slot of plane zi's (ko_x + ko_y) in s_kq (H + 1 planes deep)
 #pragma unroll
@@ -554,27 +558,24 @@ __device__ __forceinline__ void derive_item(const DerivArgs& a, const UnitDev& u
         const double kx = clx ? cl_ko(pc, 1, gi, nx, lox, hix, cx) : Rows::ko(wx, 3, cx);
         const double ky = cly ? cl_ko(pc, kPlaneW, gj, ny, loy, hiy, cy) : Rows::ko(wy, 3, cy);
         s_kq[kslot * SH::kThreads + threadIdx.x] = __dadd_rn(kx, ky);
-        put_slot<NS, ST>(a, 3 * v + 0, lp, dx);
-        put_slot<NS, ST>(a, 3 * v + 1, lp, dy);
+        const int c = col(lp);
+        sd_first[c] = (ST)dx;
+        sd_first[c + 32] = (ST)dy;
         if (DD) {
-          const int s0 = 72 + 6 * q;
-          put_slot<NS, ST>(a, s0 + 0, lp, clx ? cl_d2(pc, 1, gi, nx, lox, hix, cx) : (double)Rows::d2(wx, 3, cx));
-          put_slot<NS, ST>(a, s0 + 3, lp, cly ? cl_d2(pc, kPlaneW, gj, ny, loy, hiy, cy) : (double)Rows::d2(wy, 3, cy));
+          sd_second[c + 0 * 32] = (ST)(clx ? cl_d2(pc, 1, gi, nx, lox, hix, cx) : (double)Rows::d2(wx, 3, cx));
+          sd_second[c + 3 * 32] = (ST)(cly ? cl_d2(pc, kPlaneW, gj, ny, loy, hiy, cy) : (double)Rows::d2(wy, 3, cy));
           const double* pd = Dxp + (ty + kHalo) * kTileX + tx;
           double wd[7];
 #pragma unroll
           for (int k = 0; k < 7; ++k) wd[k] = pd[(k - 3) * kTileX];
-          put_slot<NS, ST>(a, s0 + 1, lp,
-                       cly ? cl_d1(pd, kTileX, gj, ny, loy, hiy, cy) : (double)Rows::d1(wd, 3, cy));
+          sd_second[c + 1 * 32] = (ST)(cly ? cl_d1(pd, kTileX, gj, ny, loy, hiy, cy) : (double)Rows::d1(wd, 3, cy));
         }
         if constexpr (ADV) {
           // deriv42adv_x / _y (derivs.cpp:495-775) with beta0 / beta1 at the point
           const int64_t pe = (int64_t)B.offset + gi + (int64_t)nx * gj + plane_elems * zi;
           const bool upx = __ldg(a.u[6] + pe) > 0.0, upy = __ldg(a.u[7] + pe) > 0.0;
-          put_slot<NS, ST>(a, kNumDerivs + 3 * v + 0, lp,
-                       (double)Rows::adv(wx, 3, adv_row_id(gi, nx, lox, hix, upx), cx));
-          put_slot<NS, ST>(a, kNumDerivs + 3 * v + 1, lp,
-                       (double)Rows::adv(wy, 3, adv_row_id(gj, ny, loy, hiy, upy), cy));
+          sd_adv[c] = (ST)(double)Rows::adv(wx, 3, adv_row_id(gi, nx, lox, hix, upx), cx);
+          sd_adv[c + 32] = (ST)(double)Rows::adv(wy, 3, adv_row_id(gj, ny, loy, hiy, upy), cy);
         }
       }
     }
@@ -594,23 +595,22 @@ __device__ __forceinline__ void derive_item(const DerivArgs& a, const UnitDev& u
       const LineScales& cz = s_sc[2];
       const int zc = CL ? z_case(zo, nz, loz, hiz) : -1;
       const int lp = lp_col + plane_pts * (zo - k0);
-      put_slot<NS, ST>(a, 3 * v + 2, lp, zrow_d1<CL, Rows>(qu, zc, cz));
+      const int c = col(lp);
+      sd_first[c + 2 * 32] = (ST)zrow_d1<CL, Rows>(qu, zc, cz);
       // rhs.cpp:332-369 sums (ko_x + ko_y) + ko_z
       // summed in FP64, stored like the slots (FP32 in MIXED: the term enters the output
       // scaled by sigma, far below the output's own scale)
-      static_cast<ST*>(a.koscr)[scr_index<kNumVars>(v, lp)] = (ST)__dadd_rn(kxy, zrow_ko<CL, Rows>(qu, zc, cz));
+      sk[kcol(lp)] = (ST)__dadd_rn(kxy, zrow_ko<CL, Rows>(qu, zc, cz));
       if (DD) {
-        const int s0 = 72 + 6 * q;
-        put_slot<NS, ST>(a, s0 + 5, lp, zrow_d2<CL, Rows>(qu, zc, cz));
-        put_slot<NS, ST>(a, s0 + 2, lp, zrow_d1<CL, Rows>(qx, zc, cz));
-        put_slot<NS, ST>(a, s0 + 4, lp, zrow_d1<CL, Rows>(qy, zc, cz));
+        sd_second[c + 5 * 32] = (ST)zrow_d2<CL, Rows>(qu, zc, cz);
+        sd_second[c + 2 * 32] = (ST)zrow_d1<CL, Rows>(qx, zc, cz);
+        sd_second[c + 4 * 32] = (ST)zrow_d1<CL, Rows>(qy, zc, cz);
       }
       if constexpr (ADV) {
         // deriv42adv_z (derivs.cpp:776-900) with beta2 at the point
         const int64_t pe = (int64_t)B.offset + gi + (int64_t)nx * gj + plane_elems * zo;
         const bool upz = __ldg(a.u[8] + pe) > 0.0;
-        put_slot<NS, ST>(a, kNumDerivs + 3 * v + 2, lp,
-                     (double)Rows::adv(qu, H, adv_row_id(zo, nz, loz, hiz, upz), cz));
+        sd_adv[c + 2 * 32] = (ST)(double)Rows::adv(qu, H, adv_row_id(zo, nz, loz, hiz, upz), cz);
       }
     }
   }

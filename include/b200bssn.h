@@ -134,7 +134,7 @@ typedef struct b200bssn_plan_options {
    * kernels (derivative scratch through HBM).  FP64, the upwind mode, the
    * constraints and the host-array path always use the two-pass kernels. */
   uint32_t single_pass;
-  /* Ring slots of the one-pass kernel (0: 32; each slot 3072 points, 2 MB). */
+  /* Ring slots of the one-pass kernel (0: 128; each slot 3072 points, 2 MB). */
   uint32_t ring_slots;
   /* Tile height of the two-pass derivative kernels: 16 x tile_y columns per CTA, one
    * thread per column (0: 8; also 4 or 16). */
@@ -145,6 +145,9 @@ typedef struct b200bssn_plan_options {
    * only.  0: the measured best -- 3 for FP64 with centred advection and 16x8 tiles,
    * else 1. */
   uint32_t deriv_regs;
+  /* 2: the two-pass derivative kernels give each thread two output points (y pairs of
+   * 16x16 tiles, CTAs of 128 threads), centred advection only; 0 or 1: one point. */
+  uint32_t points_per_thread;
 } b200bssn_plan_options;
 
 /* b200bssn_plan_create with explicit options (opts may be NULL). */

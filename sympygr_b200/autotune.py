@@ -12,6 +12,7 @@ for every candidate of
   without / with second derivatives, one CTA per SM more (80 / 96) or one fewer
   (128 / 168) -- with 16x8 tiles (the plans' default is the last for FP64, the first
   for MIXED);
+* output points per thread: one, or two (y pairs of 16x16 tiles in CTAs of 128 threads);
 * slab depth (staging depth along z): the z-planes per work unit of the derivative
   kernel (candidates that cut the interior into the same number of slabs are the same
   plan, so one per slab count is timed);
@@ -66,7 +67,7 @@ def time_plan(plan, rhs, u, prm, reps: int = 5, warmup: int = 2) -> float:
 # (tile_y, deriv_regs) variants of the derivative kernels built into the library
 # (deriv_regs 1: 96/128 registers for the kinds without/with second derivatives, 2: 80/96,
 # 3: 128/168)
-KERNEL_VARIANTS = [(8, 1), (4, 1), (16, 1), (8, 2), (8, 3)]
+KERNEL_VARIANTS = [(8, 1, 1), (4, 1, 1), (16, 1, 1), (8, 2, 1), (8, 3, 1), (16, 0, 2)]  # + points per thread
 
 
 def tuned_plan(ctx, blocks, precision, table, chunk_points: int = 0):
@@ -76,7 +77,7 @@ def tuned_plan(ctx, blocks, precision, table, chunk_points: int = 0):
     depths = [choice.get(b.sz[2], {}).get("slab_depth", 0) for b in blocks]
     return capi.Plan(ctx, blocks, precision, chunk_points, deriv_ctas_per_sm=table["deriv_ctas_per_sm"],
                      block_slab_depth=depths, tile_y=table.get("tile_y", 0),
-                     deriv_regs=table.get("deriv_regs", 0))
+                     deriv_regs=table.get("deriv_regs", 0), points_per_thread=table.get("points_per_thread", 0))
 
 
 def main(argv=None):
@@ -100,30 +101,30 @@ def main(argv=None):
         rhs = torch.zeros_like(u)
         pts = sum(b.ninterior for b in blocks)
         rows = []
-        for ty, regs in KERNEL_VARIANTS:
+        for ty, regs, ppt in KERNEL_VARIANTS:
             for d in depth_candidates(n):
                 for ctas in ((0, 1, 2) if args.ctas else (0,)):
                     plan = capi.Plan(ctx, blocks, prec, slab_depth=d, deriv_ctas_per_sm=ctas, tile_y=ty,
-                                     deriv_regs=regs)
+                                     deriv_regs=regs, points_per_thread=ppt)
                     ms = time_plan(plan, list(rhs), list(u), prm, args.reps)
                     plan.close()
-                    rows.append({"tile_y": ty, "deriv_regs": regs, "slab_depth": d, "deriv_ctas_per_sm": ctas,
-                                 "ms": ms, "mpts_per_s": pts / ms / 1e3})
+                    rows.append({"tile_y": ty, "deriv_regs": regs, "points_per_thread": ppt, "slab_depth": d,
+                                 "deriv_ctas_per_sm": ctas, "ms": ms, "mpts_per_s": pts / ms / 1e3})
                     print(json.dumps({"class": n, **rows[-1]}), flush=True)
         best = max(rows, key=lambda r: r["mpts_per_s"])
         nslab = lambda d: -(-(n - 6) // d)  # noqa: E731 -- slabs of the class's blocks at depth d
         dregs = 3 if prec == capi.FP64 else 1  # the plan's default split for this precision
         default = next(r for r in rows if r["tile_y"] == 8 and r["deriv_regs"] == dregs and r["deriv_ctas_per_sm"] == 0
-                       and nslab(r["slab_depth"]) == nslab(48))
+                       and r["points_per_thread"] == 1 and nslab(r["slab_depth"]) == nslab(48))
         table["classes"][str(n)] = {"blocks": c, "points": pts, "runs": rows}
-        table["choice"][str(n)] = {k: best[k] for k in ("tile_y", "deriv_regs", "slab_depth", "deriv_ctas_per_sm",
-                                                        "mpts_per_s")}
+        table["choice"][str(n)] = {k: best[k] for k in ("tile_y", "deriv_regs", "points_per_thread", "slab_depth",
+                                                        "deriv_ctas_per_sm", "mpts_per_s")}
         table["choice"][str(n)]["gain_over_default"] = best["mpts_per_s"] / default["mpts_per_s"]
         if pts > best_points[0]:
             best_points = (pts, best)
         del u, rhs
         torch.cuda.empty_cache()
-    for k in ("deriv_ctas_per_sm", "tile_y", "deriv_regs"):
+    for k in ("deriv_ctas_per_sm", "tile_y", "deriv_regs", "points_per_thread"):
         table[k] = best_points[1][k]
     # the whole batch: default knobs against the tuned table
     u, blocks = wl.two_puncture_batch_torch(wl.BATCH_SIZES, counts, seed=0, device="cuda")
@@ -138,7 +139,8 @@ def main(argv=None):
     table["batch"] = {"points": pts, "default_mpts_per_s": pts / ms_default / 1e3,
                       "tuned_mpts_per_s": pts / ms_tuned / 1e3}
     print(json.dumps({"choice": table["choice"], "batch": table["batch"],
-                      "plan_wide": {k: table[k] for k in ("deriv_ctas_per_sm", "tile_y", "deriv_regs")}}),
+                      "plan_wide": {k: table[k] for k in ("deriv_ctas_per_sm", "tile_y", "deriv_regs",
+                                                          "points_per_thread")}}),
           flush=True)
     if args.json:
         with open(args.json, "w") as f:

@@ -97,6 +97,7 @@ class PlanOptions(ctypes.Structure):
         ("ring_slots", ctypes.c_uint32),
         ("tile_y", ctypes.c_uint32),
         ("deriv_regs", ctypes.c_uint32),
+        ("points_per_thread", ctypes.c_uint32),
     ]
 
 
@@ -289,7 +290,8 @@ class Plan:
     def __init__(self, ctx: Context, blocks: Sequence[Block], precision: int = FP64,
                  chunk_points: int = 0, slab_depth: int = 0, deriv_ctas_per_sm: int = 0,
                  block_slab_depth: Sequence[int] | None = None, advective: bool = False,
-                 single_pass: bool = False, ring_slots: int = 0, tile_y: int = 0, deriv_regs: int = 0):
+                 single_pass: bool = False, ring_slots: int = 0, tile_y: int = 0, deriv_regs: int = 0,
+                 points_per_thread: int = 0):
         lib = load()
         arr = (BlockC * len(blocks))()
         for i, b in enumerate(blocks):
@@ -306,6 +308,7 @@ class Plan:
         opts.ring_slots = int(ring_slots)
         opts.tile_y = int(tile_y)
         opts.deriv_regs = int(deriv_regs)
+        opts.points_per_thread = int(points_per_thread)
         if block_slab_depth is not None:
             if len(block_slab_depth) != len(blocks):
                 raise ValueError("block_slab_depth needs one entry per block")

@@ -93,7 +93,7 @@ const void* kind_kernel(bool mixed, bool adv, bool dd, int ty, int regv) {
 int launch_derivs(b200bssn_plan* P, DerivArgs dn, DerivArgs dd, int gn, int gd, cudaStream_t s) {
   void* an[] = {&dn};
   void* ad[] = {&dd};
-  const dim3 block((unsigned)(kTileX * P->tile_y));
+  const dim3 block((unsigned)P->deriv_threads);
   CK(P->ctx, cudaLaunchKernel(P->kind_fn[0], dim3((unsigned)gn), block, an, 0, s));
   CK(P->ctx, cudaLaunchKernel(P->kind_fn[1], dim3((unsigned)gd), block, ad, 0, s));
   return B200BSSN_OK;
@@ -414,8 +414,24 @@ int b200bssn_plan_create_ex(b200bssn_ctx* ctx, const b200bssn_block* blocks, uin
   const uint32_t regs_opt = o.deriv_regs ? o.deriv_regs
                                          : (precision == B200BSSN_FP64 && !P->advective && P->tile_y == kTileY ? 3u : 1u);
   P->deriv_regs = regs_opt >= 1 && regs_opt <= 3 ? (int)regs_opt - 1 : -1;  // kernel variant
+  P->deriv_threads = kTileX * P->tile_y;
   for (int k = 0; k < 2; ++k)
     P->kind_fn[k] = kind_kernel(precision == B200BSSN_MIXED, P->advective, k == 1, P->tile_y, P->deriv_regs);
+  if (o.points_per_thread == 2) {
+    // y pairs: 16x16 tiles, 128 threads, centred advection, the pair kernels' own split
+    const bool ok = !P->advective && (o.tile_y == 0 || o.tile_y == 16) && o.deriv_regs == 0;
+    P->tile_y = 16;
+    P->deriv_threads = 128;
+    for (int k = 0; k < 2; ++k)
+      P->kind_fn[k] = !ok ? nullptr
+                          : (precision == B200BSSN_MIXED
+                                 ? (k ? (const void*)bssn_derivs_pair_kernel<float, true>
+                                      : (const void*)bssn_derivs_pair_kernel<float, false>)
+                                 : (k ? (const void*)bssn_derivs_pair_kernel<double, true>
+                                      : (const void*)bssn_derivs_pair_kernel<double, false>));
+  } else if (o.points_per_thread > 2) {
+    P->kind_fn[0] = P->kind_fn[1] = nullptr;
+  }
   if (!P->kind_fn[0] || !P->kind_fn[1]) {
     delete P;
     return B200BSSN_ERR_INVALID_ARGUMENT;
@@ -565,7 +581,7 @@ int b200bssn_plan_create_ex(b200bssn_ctx* ctx, const b200bssn_block* blocks, uin
     const bool mx = precision == B200BSSN_MIXED, adv = P->advective;
     for (int k = 0; k < 2; ++k) {
       int per_sm = 0;
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, P->kind_fn[k], kTileX * P->tile_y, 0);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, P->kind_fn[k], P->deriv_threads, 0);
       if (o.deriv_ctas_per_sm) per_sm = std::min<int>(per_sm, (int)o.deriv_ctas_per_sm);
       P->deriv_grid[k] = std::max(1, sms * std::max(1, per_sm));
     }

@@ -76,6 +76,7 @@ struct b200bssn_plan {
   int tile_y = b200bssn::kTileY;      // tile height of the derivative kernels (4, 8 or 16)
   int deriv_regs = 0;                 // register split variant of the derivative kernels
   const void* kind_fn[2] = {nullptr, nullptr};  // the derivative kind kernels (without / with DD)
+  int deriv_threads = 128;            // threads per derivative CTA
   int deriv_grid[2] = {0, 0};  // resident CTAs of the two persistent derivative kernels
   int alg_grid = 0;           // resident CTAs of the persistent staged algebra kernel (MIXED)
   // one-pass path (MIXED, centred advection): tile-slabs in launch order, the

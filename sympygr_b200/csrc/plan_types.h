@@ -53,7 +53,7 @@ struct FusedTileDev {
 };
 constexpr int kFusedSlab = 24;                               // max interior planes per tile-slab
 constexpr int kFusedSlotPts = kTileX * kTileY * kFusedSlab;  // 3072 points per ring slot
-constexpr int kFusedRingDefault = 32;                        // slots: 64 MB in MIXED
+constexpr int kFusedRingDefault = 128;                       // slots: 256 MB in MIXED
 
 struct RangeDev {
   int32_t unit;

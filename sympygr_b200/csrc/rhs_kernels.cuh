@@ -617,6 +617,216 @@ __device__ __forceinline__ void derive_item(const DerivArgs& a, const UnitDev& u
   cp_async_wait<0>();
 }
 
+// The same item with two output points per thread: a 16x16 tile in a CTA of 128
+// threads, thread (tx, tq) owning rows 2tq and 2tq+1.  The two points share one y
+// window (8 plane values instead of 14) and one D_x y window, and the per-step loop,
+// barrier, plane copy and predicate work is spread over two points; each point keeps
+// its own z queues.  Centred advection only (no upwind rows).
+template <typename ST, bool DD, bool CL = true>
+__device__ __forceinline__ void derive_item_pair(const DerivArgs& a, const UnitDev& un, const TileDev& t,
+                                                 const ScratchMap sm, const int v, double* s_plane,
+                                                 void* s_dxp_raw, double* s_kq, LineScales* s_sc) {
+  using Rows = typename RowsFor<ST>::type;
+  constexpr int NS = kNumDerivs;
+  constexpr int NT = 128, TR = 16, WARPS = NT / 32;
+  constexpr int PH = TR + 2 * kHalo, PLANE = kPlaneW * PH;  // 24 x 24 staged plane
+  constexpr int SROWS = PH / WARPS;                          // plane rows per thread
+  constexpr int DXR = TR + 2 * kHalo, DXT = DXR / (NT / kTileX);  // D_x halo rows: 24, 3 per thread
+  static_assert(SROWS * WARPS == PH && DXT * (NT / kTileX) == DXR, "pair tile geometry");
+  double* s_dxp = static_cast<double*>(s_dxp_raw);
+  const BlockDev& B = a.blocks[un.block];
+  const int nx = B.sz[0], ny = B.sz[1], nz = B.sz[2];
+  const int i0 = 3 + t.i0, j0 = 3 + t.j0, k0 = 3 + un.k0;
+  const int ex = t.ex, ey = t.ey, ez = un.nz;
+  const int ox = i0 - kHalo, oy = j0 - kHalo;
+  const int xlo = max(0, ox), xhi = min(nx, i0 + ex + kHalo);
+  const int ylo = max(0, oy), yhi = min(ny, j0 + ey + kHalo);
+  const uint32_t bf = B.bflag;
+  const bool lox = CL && (bf & 1u), hix = CL && (bf & 2u), loy = CL && (bf & 4u),
+             hiy = CL && (bf & 8u), loz = CL && (bf & 16u), hiz = CL && (bf & 32u);
+  if (threadIdx.x < 3) s_sc[threadIdx.x] = make_line_scales(B.h[threadIdx.x]);
+
+  const int tx = threadIdx.x & 15, tq = threadIdx.x >> 4, ty0 = 2 * tq;
+  const int gi = i0 + tx;
+  const bool clx = closure_row(gi, nx, lox, hix);
+  bool active[2], cly[2];
+  int gj[2], lp_col[2];
+#pragma unroll
+  for (int p = 0; p < 2; ++p) {
+    active[p] = tx < ex && ty0 + p < ey;
+    gj[p] = j0 + ty0 + p;
+    cly[p] = closure_row(gj[p], ny, loy, hiy);
+    lp_col[p] = sm.col_base + tx + sm.row_stride * (ty0 + p);
+  }
+  const bool any = active[0] || active[1];
+  const int plane_pts = sm.plane_pts;
+  constexpr int H = CL ? kHalo : 3;
+  constexpr int QD = 2 * H + 1;
+  const int zs = max(0, k0 - H);
+  const int zend = k0 + ez + H;
+  const int zload = min(nz, zend);
+
+  const int sbx = threadIdx.x & 31, sby0 = threadIdx.x >> 5;
+  int st_soff[SROWS], st_goff[SROWS];
+  bool st_ok[SROWS];
+#pragma unroll
+  for (int r = 0; r < SROWS; ++r) {
+    const int by = sby0 + WARPS * r, pi = ox + sbx, pj = oy + by;
+    st_ok[r] = sbx < kPlaneW && pi >= xlo && pi < xhi && pj >= ylo && pj < yhi;
+    st_soff[r] = by * kPlaneW + sbx;
+    st_goff[r] = pi + nx * pj;
+  }
+  const int dxx = threadIdx.x & 15, dyy0 = threadIdx.x >> 4;
+  const int dpi = i0 + dxx;
+  const bool dcl = closure_row(dpi, nx, lox, hix);
+  bool dx_ok[DXT];
+#pragma unroll
+  for (int r = 0; r < DXT; ++r) {
+    const int yy = dyy0 + (NT / kTileX) * r, pj = oy + yy;
+    dx_ok[r] = yy < DXR && dxx < ex && pj >= ylo && pj < yhi;
+  }
+  const int64_t plane_elems = (int64_t)nx * ny;
+
+  const int q = DD ? dd_index(v) : -1;
+  const double* __restrict__ f = a.u[v] + B.offset;
+  ST* const sd_first = static_cast<ST*>(a.dscr) + (3 * v) * 32;
+  ST* const sd_second = static_cast<ST*>(a.dscr) + (72 + 6 * (DD ? q : 0)) * 32;
+  ST* const sk = static_cast<ST*>(a.koscr) + v * 32;
+  auto col = [](int lp) { return (lp >> 5) * (NS * 32) + (lp & 31); };
+  auto kcol = [](int lp) { return (lp >> 5) * (kNumVars * 32) + (lp & 31); };
+  double qu[2][QD], qx[2][QD], qy[2][QD];
+  int kslot = 0;
+#pragma unroll
+  for (int p = 0; p < 2; ++p)
+#pragma unroll
+    for (int k = 0; k < QD; ++k) qu[p][k] = qx[p][k] = qy[p][k] = 0.0;
+
+  auto stage = [&](int zi, int b) {
+    const double* fp = f + plane_elems * zi;
+    const bool in = zi < zload;
+#pragma unroll
+    for (int r = 0; r < SROWS; ++r) cp_async8_if(s_plane + b * PLANE + st_soff[r], fp + st_goff[r], in && st_ok[r]);
+    cp_async_commit();
+  };
+  const LineScales& cx = s_sc[0];
+  const LineScales& cy = s_sc[1];
+  auto dx_rows = [&](int zp, const double* P, double* dst) {
+    if (zp < zload) {
+#pragma unroll
+      for (int r = 0; r < DXT; ++r) {
+        if (dx_ok[r]) {
+          const int yy = dyy0 + (NT / kTileX) * r;
+          const double* pr = P + yy * kPlaneW + dxx + kHalo;
+          double w[7];
+#pragma unroll
+          for (int k = 0; k < 7; ++k) w[k] = pr[k - 3];
+          dst[yy * kTileX + dxx] = dcl ? cl_d1(pr, 1, dpi, nx, lox, hix, cx) : Rows::d1_field(w, 3, cx);
+        }
+      }
+    }
+  };
+  stage(zs, 0);
+  stage(zs + 1, 1);
+  stage(zs + 2, 2);
+  if (DD) {
+    cp_async_wait<2>();
+    __syncthreads();
+    dx_rows(zs, s_plane, s_dxp);
+  }
+  for (int zi = zs, b = 0; zi < zend; ++zi, b = (b + 1) & 3) {
+    cp_async_wait<1>();
+    __syncthreads();
+    stage(zi + 3, (b + 3) & 3);
+    const double* P = s_plane + b * PLANE;
+    const double* Dxp = s_dxp + ((zi - zs) & 1) * (DXR * kTileX);
+    const bool in_block = zi < nz;
+    const bool out_plane = zi >= k0 && zi < k0 + ez;
+    if (DD) dx_rows(zi + 1, s_plane + ((b + 1) & 3) * PLANE, s_dxp + ((zi + 1 - zs) & 1) * (DXR * kTileX));
+
+    double u0[2] = {0.0, 0.0}, dx[2] = {0.0, 0.0}, dy[2] = {0.0, 0.0};
+    const double* pc0 = P + (ty0 + kHalo) * kPlaneW + (tx + kHalo);
+    if (any && in_block) {
+      u0[0] = active[0] ? pc0[0] : 0.0;
+      u0[1] = active[1] ? pc0[kPlaneW] : 0.0;
+    }
+    if (any && in_block && (DD || out_plane)) {
+      double wy8[8];  // rows ty0-3 .. ty0+4 of column tx: the y windows of both points
+#pragma unroll
+      for (int k = 0; k < 8; ++k) wy8[k] = pc0[(k - 3) * kPlaneW];
+      double wd8[8];  // the same rows of D_x (DD)
+      if (DD) {
+        const double* pd0 = Dxp + (ty0 + kHalo) * kTileX + tx;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) wd8[k] = pd0[(k - 3) * kTileX];
+      }
+#pragma unroll
+      for (int p = 0; p < 2; ++p) {
+        if (!active[p]) continue;
+        const double* pc = pc0 + p * kPlaneW;
+        double wx[7], wy[7];
+#pragma unroll
+        for (int k = 0; k < 7; ++k) {
+          wx[k] = pc[k - 3];
+          wy[k] = wy8[k + p];
+        }
+        dx[p] = DD ? wd8[3 + p] : (clx ? cl_d1(pc, 1, gi, nx, lox, hix, cx) : Rows::d1_field(wx, 3, cx));
+        dy[p] = cly[p] ? cl_d1(pc, kPlaneW, gj[p], ny, loy, hiy, cy) : Rows::d1_field(wy, 3, cy);
+        if (out_plane) {
+          const int lp = lp_col[p] + plane_pts * (zi - k0);
+          const double kx = clx ? cl_ko(pc, 1, gi, nx, lox, hix, cx) : Rows::ko(wx, 3, cx);
+          const double ky = cly[p] ? cl_ko(pc, kPlaneW, gj[p], ny, loy, hiy, cy) : Rows::ko(wy, 3, cy);
+          s_kq[(kslot * NT + threadIdx.x) * 2 + p] = __dadd_rn(kx, ky);
+          const int c = col(lp);
+          sd_first[c] = (ST)dx[p];
+          sd_first[c + 32] = (ST)dy[p];
+          if (DD) {
+            sd_second[c + 0 * 32] = (ST)(clx ? cl_d2(pc, 1, gi, nx, lox, hix, cx) : (double)Rows::d2(wx, 3, cx));
+            sd_second[c + 3 * 32] = (ST)(cly[p] ? cl_d2(pc, kPlaneW, gj[p], ny, loy, hiy, cy) : (double)Rows::d2(wy, 3, cy));
+            double wd[7];
+#pragma unroll
+            for (int k = 0; k < 7; ++k) wd[k] = wd8[k + p];
+            const double* pd = Dxp + (ty0 + p + kHalo) * kTileX + tx;
+            sd_second[c + 1 * 32] = (ST)(cly[p] ? cl_d1(pd, kTileX, gj[p], ny, loy, hiy, cy) : (double)Rows::d1(wd, 3, cy));
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int p = 0; p < 2; ++p) {
+      q_push(qu[p], u0[p]);
+      if (DD) {
+        q_push(qx[p], dx[p]);
+        q_push(qy[p], dy[p]);
+      }
+    }
+    const int kold = kslot == H ? 0 : kslot + 1;
+    double kxy[2];
+#pragma unroll
+    for (int p = 0; p < 2; ++p) kxy[p] = s_kq[(kold * NT + threadIdx.x) * 2 + p];
+    kslot = kold;
+
+    const int zo = zi - H;
+    if (zo >= k0 && zo < k0 + ez) {
+      const LineScales& cz = s_sc[2];
+      const int zc = CL ? z_case(zo, nz, loz, hiz) : -1;
+#pragma unroll
+      for (int p = 0; p < 2; ++p) {
+        if (!active[p]) continue;
+        const int lp = lp_col[p] + plane_pts * (zo - k0);
+        const int c = col(lp);
+        sd_first[c + 2 * 32] = (ST)zrow_d1<CL, Rows>(qu[p], zc, cz);
+        sk[kcol(lp)] = (ST)__dadd_rn(kxy[p], zrow_ko<CL, Rows>(qu[p], zc, cz));
+        if (DD) {
+          sd_second[c + 5 * 32] = (ST)zrow_d2<CL, Rows>(qu[p], zc, cz);
+          sd_second[c + 2 * 32] = (ST)zrow_d1<CL, Rows>(qx[p], zc, cz);
+          sd_second[c + 4 * 32] = (ST)zrow_d1<CL, Rows>(qy[p], zc, cz);
+        }
+      }
+    }
+  }
+  cp_async_wait<0>();
+}
+
 // Two-pass path: item (tile t of a unit, variable v) with the unit's compact scratch
 // numbering.
 template <typename ST, bool DD, bool ADV = false, bool CL = true, int TY = kTileY>
@@ -727,6 +937,38 @@ bssn_derivs_kind_kernel(const __grid_constant__ DerivArgs a) {
       derive_tile<ST, DD, ADV, true, TY>(a, t, kind_var(DD, item % NV), s_plane, s_dxp, s_kq, s_sc);
     else
       derive_tile<ST, DD, ADV, false, TY>(a, t, kind_var(DD, item % NV), s_plane, s_dxp, s_kq, s_sc);
+  }
+}
+
+// The derivative kinds with two output points per thread (derive_item_pair) on 16x16
+// tiles in CTAs of 128 threads; CTAs per SM: 3 without second derivatives, 2 with.
+constexpr int pair_ctas_per_sm(bool dd) { return dd ? 2 : 3; }
+
+template <typename ST, bool DD>
+__global__ void __launch_bounds__(128, pair_ctas_per_sm(DD))
+bssn_derivs_pair_kernel(const __grid_constant__ DerivArgs a) {
+  constexpr int NV = kKindVars[DD];
+  constexpr int PLANE = kPlaneW * (16 + 2 * kHalo);
+  __shared__ double s_plane[4 * PLANE];
+  __shared__ double s_dxp[DD ? 2 * (16 + 2 * kHalo) * kTileX : 1];
+  __shared__ double s_kq[(kHalo + 1) * 128 * 2];
+  __shared__ LineScales s_sc[3];
+  __shared__ int s_item;
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) s_item = atomicAdd(a.counter, 1);
+    __syncthreads();
+    const int item = s_item;
+    if (item >= a.tile_count * NV) break;
+    const TileDev t = a.tiles[a.tile_base + item / NV];
+    const UnitDev un = a.units[t.unit];
+    const int I0 = a.blocks[un.block].sz[0] - 6, I1 = a.blocks[un.block].sz[1] - 6;
+    const ScratchMap sm{(int)un.sbase + t.i0 + I0 * t.j0, I0, I0 * I1};
+    const int v = kind_var(DD, item % NV);
+    if (item_has_closure(a.blocks[un.block], un, t))
+      derive_item_pair<ST, DD, true>(a, un, t, sm, v, s_plane, s_dxp, s_kq, s_sc);
+    else
+      derive_item_pair<ST, DD, false>(a, un, t, sm, v, s_plane, s_dxp, s_kq, s_sc);
   }
 }
 

@@ -45,7 +45,7 @@ def test_every_declared_function_is_exported(lib):
 def test_struct_layouts_match_c(tmp_path):
     src = tmp_path / "layout.c"
     src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "b200bssn.h"\n'
-                   'int main(void){printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\\n", sizeof(b200bssn_params),'
+                   'int main(void){printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\\n", sizeof(b200bssn_params),'
                    ' offsetof(b200bssn_params, precision), sizeof(b200bssn_block),'
                    ' offsetof(b200bssn_block, pmin), sizeof(b200bssn_plan_options),'
                    ' offsetof(b200bssn_plan_options, deriv_ctas_per_sm),'
@@ -54,7 +54,8 @@ def test_struct_layouts_match_c(tmp_path):
                    ' offsetof(b200bssn_plan_options, single_pass),'
                    ' offsetof(b200bssn_plan_options, ring_slots),'
                    ' offsetof(b200bssn_plan_options, tile_y),'
-                   ' offsetof(b200bssn_plan_options, deriv_regs)); return 0;}\n')
+                   ' offsetof(b200bssn_plan_options, deriv_regs),'
+                   ' offsetof(b200bssn_plan_options, points_per_thread)); return 0;}\n')
     exe = tmp_path / "layout"
     subprocess.run(["gcc", "-I", os.path.join(REPO, "include"), str(src), "-o", str(exe)], check=True)
     got = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True,
@@ -64,7 +65,7 @@ def test_struct_layouts_match_c(tmp_path):
             capi.PlanOptions.deriv_ctas_per_sm.offset, capi.PlanOptions.block_slab_depth.offset,
             capi.PlanOptions.advective.offset, capi.PlanOptions.single_pass.offset,
             capi.PlanOptions.ring_slots.offset, capi.PlanOptions.tile_y.offset,
-            capi.PlanOptions.deriv_regs.offset]
+            capi.PlanOptions.deriv_regs.offset, capi.PlanOptions.points_per_thread.offset]
     assert got == want
 
 

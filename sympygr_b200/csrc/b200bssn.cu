@@ -614,7 +614,7 @@ int b200bssn_plan_create_ex(b200bssn_ctx* ctx, const b200bssn_block* blocks, uin
       return (int64_t)B.sz[0] * B.sz[1] * B.sz[2];
     };
     std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) { return npad(x) > npad(y); });
-    int64_t groups = 0;
+    int64_t groups = 0;  // planes over all tile-slabs (algebra work units)
     for (uint32_t b : order) {
       const BlockDev& B = P->blocks[b];
       const int I0 = B.sz[0] - 6, I1 = B.sz[1] - 6, I2 = B.sz[2] - 6;
@@ -631,7 +631,7 @@ int b200bssn_plan_create_ex(b200bssn_ctx* ctx, const b200bssn_block* blocks, uin
             t.ey = (int16_t)std::min(kTileY, I1 - j0);
             t.k0 = (int16_t)k0;
             t.nz = (int16_t)(k1 - k0);
-            t.group_base = (int32_t)std::min<int64_t>(groups, INT32_MAX);
+            t.pad = 0;
             groups += t.nz;
             P->ftiles.push_back(t);
           }
@@ -641,7 +641,6 @@ int b200bssn_plan_create_ex(b200bssn_ctx* ctx, const b200bssn_block* blocks, uin
       delete P;
       return B200BSSN_ERR_SIZE_LIMIT;
     }
-    P->ngroups = (int32_t)groups;
     P->fsync_words = 4 + 3 * P->ftiles.size() + (size_t)P->nring;
     int sms = 0, per_sm = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);

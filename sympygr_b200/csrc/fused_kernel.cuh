@@ -1,6 +1,9 @@
 // Single-pass right-hand side: one persistent kernel for a whole evaluation, with
-// the derivative scratch kept in a ring of tile-slab slots small enough to stay in
-// the 126 MB L2 instead of a full scratch array in HBM.
+// the derivative scratch in a ring of tile-slab slots instead of a full scratch array
+// in HBM: each slot is reused as soon as its tile-slab's algebra is done, so the lines
+// written are read back (mostly from L2) while they are fresh.  The default ring has
+// 128 slots (256 MB); 32 slots (64 MB) fit the 126 MB L2 but leave items waiting for
+// free slots (measured slower).
 //
 // Work units (plan order, see b200bssn.cu):
 //   tile-slab T  a 16x8 column tile of a block over a z-slab of at most kFusedSlab
@@ -41,7 +44,7 @@
 
 namespace b200bssn {
 
-constexpr int kFusedThreads = 128;                              // 4 warps: one derivative item or one group
+constexpr int kFusedThreads = 128;                              // 4 warps: one item or one algebra claim
 constexpr int kFusedMinBlocks = 3;                              // CTAs per SM (168 registers)
 constexpr unsigned long long kFusedWaitNs = 2000000000ull;      // 2 s per wait, then an error
 constexpr size_t kFusedStageBytes = (size_t)kNumDerivs * kStageW * sizeof(float);  // per warp

@@ -82,7 +82,7 @@ struct b200bssn_plan {
   // one-pass path (MIXED, centred advection): tile-slabs in launch order, the
   // per-evaluation sync words and the scratch ring
   bool single_pass = false;
-  int32_t nring = 0, ngroups = 0, fused_grid = 0;
+  int32_t nring = 0, fused_grid = 0;
   std::vector<b200bssn::FusedTileDev> ftiles;
   void* fdesc = nullptr;
   b200bssn::FusedTileDev* d_ftiles = nullptr;

@@ -49,7 +49,7 @@ struct FusedTileDev {
   int16_t i0, j0;     // interior-relative x-y origin of the tile
   int16_t ex, ey;     // extents (<= kTileX, kTileY)
   int16_t k0, nz;     // interior-relative first plane and planes (<= kFusedSlab)
-  int32_t group_base; // first algebra group of the tile-slab (one group per plane)
+  int32_t pad;
 };
 constexpr int kFusedSlab = 24;                               // max interior planes per tile-slab
 constexpr int kFusedSlotPts = kTileX * kTileY * kFusedSlab;  // 3072 points per ring slot

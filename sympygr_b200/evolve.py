@@ -15,8 +15,14 @@ Sommerfeld values (bssn/src/rhs.cpp:833-977):
 On faces inside the strong-field region the reference's closure + Sommerfeld
 treatment grows exponentially (its own right-hand side shows it: K grows ~2.5x every
 5 steps next to one flagged face of a 37^3 block, at any KO strength), so the
-100-step comparison runs with ``frozen``; the other two modes show that growth
-and that mixed precision follows FP64 through it.  dt = CFL * the smallest spacing.  The whole step loop runs as replays of a CUDA graph of
+100-step comparison of the batch runs with ``frozen``; the other two modes show that
+growth and that mixed precision follows FP64 through it.
+
+``--layout tiled`` evolves instead a cube domain [-L, L]^3 (``--half-width``) tiled
+by ``--tiles``^3 blocks of padded size ``--tile-size`` around the same two punctures:
+the faces on the domain boundary carry the Sommerfeld values and one-sided closures
+(their bflag bits), the faces between blocks keep the frozen initial ghost data (the
+ghost exchange between blocks is outside this path).  dt = CFL * the smallest spacing.  The whole step loop runs as replays of a CUDA graph of
 ``--graph-steps`` RK4 steps (each step: 4 stages x 3 launches per chunk, the stage
 update fused into the algebra kernel).  Every ``--check-every`` steps the driver
 evaluates the Hamiltonian and momentum constraints on the device (per-block sums of
@@ -197,7 +203,12 @@ def main(argv=None):
     ap.add_argument("--graph-steps", type=int, default=10)
     ap.add_argument("--chunk-points", type=int, default=0)
     ap.add_argument("--precisions", default="fp64,mixed")
-    ap.add_argument("--boundary", default="frozen", choices=["frozen", "batch", "all"])
+    ap.add_argument("--boundary", default="frozen", choices=["frozen", "batch", "all"],
+                    help="face flags of the batch layout")
+    ap.add_argument("--layout", default="batch", choices=["batch", "tiled"])
+    ap.add_argument("--tiles", type=int, default=4, help="tiled layout: blocks per axis")
+    ap.add_argument("--tile-size", type=int, default=37, help="tiled layout: padded block size")
+    ap.add_argument("--half-width", type=float, default=8.0, help="tiled layout: domain [-L, L]^3")
     ap.add_argument("--checkpoint", default="", help="directory for the final states")
     ap.add_argument("--resume", default="", help="checkpoint directory of one precision to continue")
     ap.add_argument("--json", default="")
@@ -212,6 +223,11 @@ def main(argv=None):
         dt = float(meta["dt"])
         args.precisions = meta["precision"]
         args.boundary = meta["boundary"]
+    elif args.layout == "tiled":
+        blocks, total = wl.tiled_domain_blocks(args.tiles, args.tile_size, args.half_width)
+        u0 = wl.two_puncture_fields_torch(blocks, total, device="cuda")
+        args.boundary = "domain"
+        dt = args.cfl * min(min(b.h) for b in blocks)
     else:
         u0, blocks = wl.two_puncture_batch_torch(wl.BATCH_SIZES, scaled_counts(args.scale), args.seed,
                                                  device="cuda")
@@ -226,7 +242,12 @@ def main(argv=None):
         nx, ny, nz = b.sz
         seg = mask[b.offset:b.offset + b.npad].view(nz, ny, nx)
         seg[3:-3, 3:-3, 3:-3] = True
-    out = {"workload": f"two-puncture batch x{args.scale:g}, {len(blocks)} blocks",
+    if args.layout == "tiled" and not args.resume:
+        workload = (f"two-puncture tiled domain [-{args.half_width:g}, {args.half_width:g}]^3, "
+                    f"{args.tiles}^3 blocks of {args.tile_size}^3")
+    else:
+        workload = f"two-puncture batch x{args.scale:g}, {len(blocks)} blocks"
+    out = {"workload": workload,
            "boundary": args.boundary,
            "points": sum(b.ninterior for b in blocks), "dt": dt, "cfl": args.cfl,
            "probes": [{"target": t, "point": p[1]} for t, p in zip(PUNCTURES, probes)],

@@ -23,6 +23,10 @@ Workloads (seeded, no external data):
                      softened as above, alpha=chi^(1/2), gt=delta, the rest 0);
                      10 % of the blocks get a random non-zero face mask.  Block
                      starts are aligned to 32 elements.
+* ``tiled_domain_blocks`` blocks of one padded size tiling a cube domain around the
+                     same two punctures, the domain's outer faces flagged (Sommerfeld)
+                     and the faces between blocks not: the layout of an evolution whose
+                     only physical boundary is the outer one.
 """
 from __future__ import annotations
 
@@ -149,13 +153,39 @@ def two_puncture_batch(sizes=BATCH_SIZES, counts=BATCH_COUNTS, seed: int = 0):
     return u, blocks
 
 
-def two_puncture_batch_torch(sizes=BATCH_SIZES, counts=BATCH_COUNTS, seed: int = 0,
-                             device="cuda"):
-    """Same data as ``two_puncture_batch`` built with torch on `device` (fast for
-    the full 1.4e8-point batch).  Returns (u tensor [24, total], blocks)."""
+def tiled_domain_blocks(ntile: int = 4, n: int = 37, half_width: float = 8.0, align: int = 32):
+    """Blocks of padded size n^3 tiling the cube [-half_width, half_width]^3 with
+    ntile^3 blocks: the interiors ((n-6)^3 points each) abut with one spacing h between
+    neighbouring interior points, and each block's bflag marks exactly its faces on the
+    domain boundary (bits x-, x+, y-, y+, z-, z+ as in the reference's def.h), so the
+    Sommerfeld values apply on the outer boundary only.  Returns (blocks, total)."""
+    interior = n - 6
+    width = 2.0 * half_width / ntile
+    h = width / interior
+    blocks, off = [], 0
+    for bz in range(ntile):
+        for by in range(ntile):
+            for bx in range(ntile):
+                lo = [-half_width + c * width for c in (bx, by, bz)]
+                flag = 0
+                for a, c in enumerate((bx, by, bz)):
+                    if c == 0:
+                        flag |= 1 << (2 * a)
+                    if c == ntile - 1:
+                        flag |= 1 << (2 * a + 1)
+                pmin = tuple(lo[a] - 3 * h for a in range(3))
+                pmax = tuple(pmin[a] + (n - 1) * h for a in range(3))
+                blocks.append(Block(off, (n, n, n), flag, pmin, pmax))
+                off += ((n ** 3 + align - 1) // align) * align
+    return blocks, off
+
+
+def two_puncture_fields_torch(blocks, total: int, device="cuda"):
+    """The two-puncture Brill-Lindquist fields (m = 0.5 at x = +-4, softened, alpha =
+    chi^(1/2), gt = delta, the rest 0) at every padded point of the given blocks,
+    built with torch on `device`: a [24, total] tensor."""
     import torch
 
-    blocks, total = batch_blocks(sizes, counts, seed)
     u = torch.zeros((NUM_VARS, total), dtype=torch.float64, device=device)
     for v in (U_SYMGT0, U_SYMGT3, U_SYMGT5):
         u[v].fill_(1.0)  # gaps between blocks hold flat values too; never read
@@ -187,7 +217,15 @@ def two_puncture_batch_torch(sizes=BATCH_SIZES, counts=BATCH_COUNTS, seed: int =
             flat = (idx[:, None] + torch.arange(n ** 3, device=device)[None, :]).reshape(-1)
             u[U_CHI].index_copy_(0, flat, chi.reshape(-1))
             u[U_ALPHA].index_copy_(0, flat, alpha.reshape(-1))
-    return u, blocks
+    return u
+
+
+def two_puncture_batch_torch(sizes=BATCH_SIZES, counts=BATCH_COUNTS, seed: int = 0,
+                             device="cuda"):
+    """Same data as ``two_puncture_batch`` built with torch on `device` (fast for
+    the full 1.4e8-point batch).  Returns (u tensor [24, total], blocks)."""
+    blocks, total = batch_blocks(sizes, counts, seed)
+    return two_puncture_fields_torch(blocks, total, device), blocks
 
 
 def interior_mask(blk: Block):

@@ -146,3 +146,18 @@ def test_evolve_checkpoint_resume_is_bitwise(tmp_path):
     assert np.array_equal(sa, sc)
     assert out["runs"]["fp64"]["finite"]
     assert out["runs"]["fp64"]["history"][-1]["step"] == 4
+
+
+def test_evolve_tiled_domain_with_sommerfeld_faces(tmp_path):
+    """A cube domain tiled by 2^3 blocks, Sommerfeld faces on its outer boundary only:
+    both precisions stay finite and mixed follows FP64."""
+    from sympygr_b200 import evolve
+
+    out = evolve.main(["--layout", "tiled", "--tiles", "2", "--tile-size", "21", "--half-width", "8",
+                       "--steps", "6", "--check-every", "3", "--graph-steps", "3",
+                       "--json", str(tmp_path / "t.json")])
+    assert out["boundary"] == "domain"
+    for name in ("fp64", "mixed"):
+        assert out["runs"][name]["finite"] and out["runs"][name]["steps"] == 6
+    assert max(c["max_rel"] for c in out["mixed_vs_fp64_change"]) < 1e-4
+    assert abs(out["ham_growth_ratio_mixed_over_fp64"] - 1.0) < 1e-3

@@ -100,8 +100,9 @@ const char *b200bssn_status_string(int status);
 
 /* Drop-in for bssnrhs (bssn/include/rhs.h:33-36): one block, HOST arrays.
  * rhs[v] and u[v] (v < 24) are the caller's zipped arrays; the block's slice is
- * copied to the device, evaluated, and its interior copied back.  Blocks until
- * the result is in `rhs`. */
+ * copied to the device, evaluated, and its interior copied back, both through a
+ * pinned host buffer the context keeps (24 x the block's points, grown on
+ * demand; host threads do the copies).  Blocks until the result is in `rhs`. */
 int b200bssn_rhs(b200bssn_ctx *ctx, double *const *rhs, const double *const *u,
                  uint32_t offset, const double *pmin, const double *pmax,
                  const uint32_t *sz, uint32_t bflag, const b200bssn_params *prm);

@@ -3,9 +3,12 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <system_error>
+#include <thread>
 #include <vector>
 
 #include "b200bssn.h"
@@ -370,6 +373,9 @@ int b200bssn_destroy(b200bssn_ctx* ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   cudaFree(ctx->blk_u);
   cudaFree(ctx->blk_rhs);
+  cudaFreeHost(ctx->blk_pin);
+  for (cudaEvent_t e : ctx->blk_ev)
+    if (e) cudaEventDestroy(e);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   if (ctx->s_deriv) cudaStreamDestroy(ctx->s_deriv);
   if (ctx->s_alg) cudaStreamDestroy(ctx->s_alg);
@@ -921,6 +927,50 @@ int b200bssn_rhs_plan_host(b200bssn_plan* P, double* const* rhs, const double* c
 
 namespace {
 
+// Host threads for staging `bytes` of block data: one per 4 MB, at most 8 and at
+// most the host's hardware threads.
+int staging_threads(size_t bytes) {
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  return (int)std::min<size_t>({8, hw, bytes / (4u << 20) + 1});
+}
+
+// Runs fn(i) for i in [0, n) on up to `threads` host threads (the calling thread
+// among them; each worker selects `device` first) and returns the first CUDA error.
+// Workers that cannot be started leave their share to the others.
+template <class F>
+cudaError_t host_parallel(int device, int n, int threads, F fn) {
+  std::atomic<int> next{0};
+  std::atomic<int> err{(int)cudaSuccess};
+  auto work = [&](bool worker) {
+    if (worker) {
+      const cudaError_t e = cudaSetDevice(device);
+      if (e != cudaSuccess) {
+        int ok = (int)cudaSuccess;
+        err.compare_exchange_strong(ok, (int)e);
+        return;
+      }
+    }
+    for (int i; (i = next.fetch_add(1)) < n;) {
+      const cudaError_t e = fn(i);
+      if (e != cudaSuccess) {
+        int ok = (int)cudaSuccess;
+        err.compare_exchange_strong(ok, (int)e);
+      }
+    }
+  };
+  std::vector<std::thread> pool;
+  for (int t = 1; t < std::min(threads, n); ++t) {
+    try {
+      pool.emplace_back(work, true);
+    } catch (const std::system_error&) {
+      break;
+    }
+  }
+  work(false);
+  for (std::thread& t : pool) t.join();
+  return (cudaError_t)err.load();
+}
+
 // Single-block path shared by the drop-in entry points: (re)builds the one-block
 // plan when the size or precision changes (otherwise only the block descriptor is
 // refreshed), sizes the block buffers and uploads the block's state.  On return
@@ -968,32 +1018,66 @@ int prepare_block(b200bssn_ctx* ctx, const double* const* u, uint32_t offset, co
     CK(ctx, cudaMalloc((void**)&ctx->blk_rhs, kNumVars * npad * sizeof(double)));
     ctx->blk_cap = npad;
   }
+  if (ctx->blk_pin_cap < kNumVars * npad) {
+    CK(ctx, cudaFreeHost(ctx->blk_pin));
+    ctx->blk_pin = nullptr;
+    ctx->blk_pin_cap = 0;
+    CK(ctx, cudaHostAlloc((void**)&ctx->blk_pin, kNumVars * npad * sizeof(double),
+                          cudaHostAllocDefault));
+    ctx->blk_pin_cap = kNumVars * npad;
+  }
   for (int v = 0; v < kNumVars; ++v) {
     ud[v] = ctx->blk_u + v * npad;
     rd[v] = ctx->blk_rhs + v * npad;
-    CK(ctx, cudaMemcpyAsync((void*)ud[v], u[v] + offset, npad * sizeof(double),
-                            cudaMemcpyHostToDevice, ctx->stream));
   }
+  // each variable goes through the pinned buffer; its upload is queued as soon as
+  // its host copy is done, so the DMA of one variable overlaps the copy of the next
+  double* pin = ctx->blk_pin;
+  double* dev = ctx->blk_u;
+  cudaStream_t s = ctx->stream;
+  const size_t bytes = npad * sizeof(double);
+  const cudaError_t e = host_parallel(
+      ctx->device, kNumVars, staging_threads(kNumVars * bytes), [=](int v) {
+        std::memcpy(pin + v * npad, u[v] + offset, bytes);
+        return cudaMemcpyAsync(dev + v * npad, pin + v * npad, bytes, cudaMemcpyHostToDevice, s);
+      });
+  if (e != cudaSuccess) return fail_cuda(ctx, e, "block upload");
   return B200BSSN_OK;
 }
 
 // Copies the interior box [3, n-3)^3 of `nout` device arrays back to the caller's
 // host arrays at `offset`; ghost points of the destination are left untouched, as
-// the reference leaves them.
+// the reference leaves them.  Each variable's interior planes come down as one
+// contiguous copy into the pinned buffer, and host threads scatter its interior rows
+// as soon as its copy is done.
 int copy_interior_back(b200bssn_ctx* ctx, double* const* dst, double* const* src, int nout,
                        uint32_t offset, const uint32_t* sz) {
-  const size_t nx = sz[0], ny = sz[1];
+  const size_t nx = sz[0], ny = sz[1], nz = sz[2];
+  const size_t plane = nx * ny, npad = plane * nz;
+  const size_t lo = 3 * plane, n = (nz - 6) * plane;
   for (int v = 0; v < nout; ++v) {
-    cudaMemcpy3DParms cp;
-    std::memset(&cp, 0, sizeof(cp));
-    cp.srcPtr = make_cudaPitchedPtr(src[v], nx * sizeof(double), nx, ny);
-    cp.dstPtr = make_cudaPitchedPtr(dst[v] + offset, nx * sizeof(double), nx, ny);
-    cp.srcPos = make_cudaPos(3 * sizeof(double), 3, 3);
-    cp.dstPos = cp.srcPos;
-    cp.extent = make_cudaExtent((nx - 6) * sizeof(double), ny - 6, sz[2] - 6);
-    cp.kind = cudaMemcpyDeviceToHost;
-    CK(ctx, cudaMemcpy3DAsync(&cp, ctx->stream));
+    if (!ctx->blk_ev[v]) CK(ctx, cudaEventCreateWithFlags(&ctx->blk_ev[v], cudaEventDisableTiming));
+    CK(ctx, cudaMemcpyAsync(ctx->blk_pin + v * npad + lo, src[v] + lo, n * sizeof(double),
+                            cudaMemcpyDeviceToHost, ctx->stream));
+    CK(ctx, cudaEventRecord(ctx->blk_ev[v], ctx->stream));
   }
+  const double* pin = ctx->blk_pin;
+  const cudaEvent_t* ev = ctx->blk_ev;
+  const size_t row = (nx - 6) * sizeof(double);
+  const cudaError_t e = host_parallel(
+      ctx->device, nout, staging_threads(nout * n * sizeof(double)), [=](int v) {
+        const cudaError_t es = cudaEventSynchronize(ev[v]);
+        if (es != cudaSuccess) return es;
+        const double* from = pin + v * npad;
+        double* to = dst[v] + offset;
+        for (size_t k = 3; k < nz - 3; ++k)
+          for (size_t j = 3; j < ny - 3; ++j) {
+            const size_t at = k * plane + j * nx + 3;
+            std::memcpy(to + at, from + at, row);
+          }
+        return cudaSuccess;
+      });
+  if (e != cudaSuccess) return fail_cuda(ctx, e, "block download");
   CK(ctx, cudaStreamSynchronize(ctx->stream));
   return B200BSSN_OK;
 }

@@ -34,6 +34,11 @@ struct b200bssn_ctx {
   b200bssn_plan* blk_plan = nullptr;
   uint32_t blk_sz[3] = {0, 0, 0};
   uint32_t blk_precision = 0xffffffffu;
+  // pinned host staging of the block's state (upload) and results (download), and
+  // one event per variable marking its download done
+  double* blk_pin = nullptr;
+  size_t blk_pin_cap = 0;  // doubles
+  cudaEvent_t blk_ev[b200bssn::kNumVars] = {};
 };
 
 struct ChunkRec {

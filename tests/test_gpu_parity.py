@@ -49,6 +49,33 @@ def test_dropin_vs_oracle_fake(ctx, oracle_lib, n, bflag):
     assert mx.max() < TOL64, (mx.max(), int(np.argmax(mx)))
 
 
+def test_dropin_offsets_and_staging_reuse(ctx, oracle_lib):
+    """Three blocks zipped into one set of arrays, evaluated one by one through the
+    drop-in in an order that grows the context's staging buffers and then reuses them
+    for a smaller block (the 70^3 block's 66 MB are staged by several host threads):
+    each call writes its block's interior and nothing else."""
+    sizes, flags = (21, 70, 45), (0x15, 0x00, 0x2A)
+    offsets = np.cumsum((0,) + tuple(n ** 3 for n in sizes))
+    u = np.zeros((24, int(offsets[-1])))
+    blocks = []
+    for n, bf, off in zip(sizes, flags, offsets):
+        ub, b = po.fake_block(n, (-0.4, 0.1, -0.2), 1.1 / n, bf)
+        u[:, off:off + n ** 3] = ub
+        blocks.append(wl.Block(int(off), b.sz, bf, b.pmin, b.pmax))
+    rhs = np.full_like(u, np.nan)
+    prm = sg.Params.make(ko_sigma=0.3)
+    written = np.zeros(u.shape[1], dtype=bool)
+    for b in (blocks[0], blocks[1], blocks[2]):
+        ctx.bssnrhs(list(rhs), list(u), b.offset, b.pmin, b.pmax, b.sz, b.bflag, prm)
+        written[b.offset:b.offset + b.npad] |= wl.interior_mask(b).ravel()
+        assert np.isnan(rhs[:, ~written]).all()
+        assert not np.isnan(rhs[:, written]).any()
+    for b in blocks:
+        ref = po.interior(po.oracle_rhs(u, b, po.params(ko_sigma=0.3)), b)
+        mx, _ = po.rel_errors(po.interior(rhs, b), ref)
+        assert mx.max() < TOL64, (b.sz, mx.max())
+
+
 def test_cfg1_sines_vs_golden(ctx, golden_dir):
     g = np.load(os.path.join(golden_dir, "sines_38.npz"))
     u, blk = wl.flat_sines(38, 0.1, 0)

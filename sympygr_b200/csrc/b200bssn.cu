@@ -550,7 +550,6 @@ int b200bssn_plan_create_ex(b200bssn_ctx* ctx, const b200bssn_block* blocks, uin
   // chunks' blocks are disjoint and in increasing offset order.
   {
     std::vector<uint64_t> lo(P->chunks.size(), UINT64_MAX), hi(P->chunks.size(), 0);
-    size_t ci = 0;
     for (size_t c = 0; c < P->chunks.size(); ++c) {
       const ChunkRec& ch = P->chunks[c];
       for (int r = ch.range_begin; r < ch.range_begin + ch.range_count; ++r) {
@@ -560,7 +559,6 @@ int b200bssn_plan_create_ex(b200bssn_ctx* ctx, const b200bssn_block* blocks, uin
         hi[c] = std::max(hi[c], B.offset + np);
       }
     }
-    (void)ci;
     bool ok = P->chunks.size() > 1;
     for (size_t c = 0; ok && c + 1 < P->chunks.size(); ++c) ok = hi[c] <= lo[c + 1];
     if (ok) {

@@ -338,9 +338,92 @@ def main_advective(args):
     print("wrote", CUDA_ADV_OUT, "and", C_ADV_OUT)
 
 
+CUDA_SPLIT_HEADER = """\
+// GENERATED by sympygr_b200/codegen/gen_bssn_rhs.py --split -- do not edit by hand.
+//
+// The per-point BSSN right-hand side of bssn_rhs_algebra.cuh partitioned by output,
+// as the reference's staged bssnrhs_sep (bssn/src/rhs.cpp:392-825) partitions its
+// loops: part 0 writes the six At_rhs (the only outputs that need the Ricci
+// tensor), part 1 the other 18.  Each part carries only the stages its outputs use
+// (the staged capture of sympygr_b200/codegen/staged.py, pruned backwards from the
+// outputs) and is CSE'd on its own, so the live set of either is a fraction of the
+// whole: a register-pressure split for the FP64 algebra.  Part 0: %(nops0)d ops,
+// %(ntmp0)d temporaries; part 1: %(nops1)d ops, %(ntmp1)d temporaries.
+// Interface as bssn_rhs_algebra; part 0 needs no parameters and no eta.
+#pragma once
+
+#include "bssn_rhs_algebra.cuh"
+
+namespace b200bssn {
+
+template <int PART>
+struct RhsAlgebraPart;
+"""
+
+# outputs of the first part of the split algebra (the Ricci-dependent ones)
+SPLIT_PART0 = ["At_rhs00", "At_rhs01", "At_rhs02", "At_rhs11", "At_rhs12", "At_rhs22"]
+CUDA_SPLIT_OUT = os.path.join(REPO, "sympygr_b200", "csrc", "generated", "bssn_rhs_algebra_split.cuh")
+
+
+def prune_stages(stages, outputs):
+    """The staged capture restricted to the named outputs: the last stage keeps only
+    those outputs, every earlier stage only the values something kept still reads
+    (walked backwards from the outputs)."""
+    out_name, out_defs = stages[-1]
+    keep = [(n, e) for n, e in out_defs if str(n) in outputs]
+    need = set()
+    for _, e in keep:
+        need |= e.free_symbols
+    pruned = []
+    for name, defs in reversed(stages[:-1]):
+        kept = [(s, e) for s, e in defs if s in need]
+        for _, e in kept:
+            need |= e.free_symbols
+        if kept:
+            pruned.append((name, kept))
+    pruned.reverse()
+    pruned.append((out_name, keep))
+    return pruned
+
+
+def main_split(args):
+    """The two-part algebra (bssn_rhs_algebra_split.cuh) from the staged capture."""
+    from .staged import capture_staged
+
+    CudaPrinter, _ = make_printers(src.load_dendro_c_printer(args.reference))
+    slots = src.derivative_slots()
+    stages = capture_staged(args.reference)
+    if args.split_ricci:
+        # the Ricci stage CSE'd in two halves (R00 R01 R02 / R11 R12 R22): a smaller
+        # live set at the price of the subexpressions the halves share
+        at = [i for i, st in enumerate(stages) if st[0] == "R"][0]
+        defs = stages[at][1]
+        stages = stages[:at] + [("R_a", defs[:3]), ("R_b", defs[3:])] + stages[at + 1:]
+    parts = [SPLIT_PART0, [n for n in src.RHS_NAMES if n not in SPLIT_PART0]]
+    texts, stats = [], {}
+    for p, outs in enumerate(parts):
+        body, nops, ntmp = emit_staged(prune_stages(stages, set(outs)), CudaPrinter(), slots)
+        stats["nops%d" % p], stats["ntmp%d" % p] = nops, ntmp
+        texts.append(
+            "template <>\nstruct RhsAlgebraPart<%d> {\n"
+            "  template <typename RT, class In, class Sink>\n"
+            "  static __device__ __forceinline__ void run(const In& in, Sink& sink,\n"
+            "                                             const AlgebraParams<RT>& prm, const RT eta) {\n"
+            "%s\n  }\n};\n" % (p, "\n".join("  " + line for line in body)))
+    with open(CUDA_SPLIT_OUT, "w") as f:
+        f.write(CUDA_SPLIT_HEADER % stats)
+        f.write("\n".join(texts))
+        f.write("\n}  // namespace b200bssn\n")
+    print("wrote", CUDA_SPLIT_OUT, stats)
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", required=True, help="root of the SymPyGR checkout")
+    ap.add_argument("--split", action="store_true",
+                    help="write only the two-part algebra (At_rhs / the rest) for the FP64 kernels")
+    ap.add_argument("--split-ricci", action="store_true",
+                    help="with --split: CSE the Ricci stage in two halves")
     ap.add_argument("--cache", default=None, help="optional pickle to reuse the CSE")
     ap.add_argument("--flat-cuda", action="store_true",
                     help="print the CUDA algebra from the single global CSE (as the C oracle)")
@@ -349,6 +432,8 @@ def main(argv=None):
     args = ap.parse_args(argv)
     if args.advective:
         return main_advective(args)
+    if args.split:
+        return main_split(args)
 
     t0 = time.time()
     if args.cache and os.path.exists(args.cache):

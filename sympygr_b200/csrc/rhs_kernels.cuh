@@ -26,6 +26,7 @@
 
 #include "generated/bssn_rhs_algebra.cuh"
 #include "generated/bssn_rhs_algebra_adv.cuh"
+#include "generated/bssn_rhs_algebra_split.cuh"
 #include "plan_types.h"
 #include "stencils.cuh"
 
@@ -1086,6 +1087,9 @@ __device__ __forceinline__ void prefetch_l2_bulk(const void* p, uint32_t bytes) 
   asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
 }
 
+// FP64 algebra as the two-part split of bssn_rhs_algebra_split.cuh
+constexpr bool kSplitAlgebra64 = true;
+
 // The right-hand side of interior point (i, j, k) (padded coordinates) of block B,
 // inputs through `src`.
 template <typename RT, int MODE, class Src, bool ADV = false>
@@ -1133,10 +1137,16 @@ __device__ __forceinline__ void algebra_point_at(const AlgebraArgs& a, const Blo
     prm = &a.prm64;
   else
     prm = &a.prm32;
-  if constexpr (ADV)
+  if constexpr (ADV) {
     bssn_rhs_algebra_adv<RT>(in, sink, *prm, (RT)eta);
-  else
+  } else if constexpr (sizeof(RT) == 8 && kSplitAlgebra64) {
+    // FP64: the algebra in two parts (the six At_rhs with the Ricci tensor, then the
+    // rest), each with its own live set
+    RhsAlgebraPart<0>::run<RT>(in, sink, *prm, (RT)eta);
+    RhsAlgebraPart<1>::run<RT>(in, sink, *prm, (RT)eta);
+  } else {
     bssn_rhs_algebra<RT>(in, sink, *prm, (RT)eta);
+  }
 }
 
 // The same for interior point lpu (compact numbering) of unit `un`.

@@ -2,7 +2,8 @@
 // bssn_rhs_algebra.cuh; with a second argument "con" the constraint algebra
 // bssn_constraints_algebra.cuh; "adv" the upwind-mode algebra bssn_rhs_algebra_adv.cuh;
 // "advsame" the oracle's upwind-mode algebra fed its advective slots from the centred
-// first derivatives, against the oracle's standard algebra) next to the oracle's C
+// first derivatives, against the oracle's standard algebra; "split" the two-part
+// algebra bssn_rhs_algebra_split.cuh, both parts in turn) next to the oracle's C
 // functions, at seeded random points. Prints the largest norm-wise relative difference
 // per output over all points.
 #include <cmath>
@@ -16,6 +17,7 @@ using std::sqrt;
 #include "bssn_constraints_algebra.cuh"
 #include "bssn_rhs_algebra.cuh"
 #include "bssn_rhs_algebra_adv.cuh"
+#include "bssn_rhs_algebra_split.cuh"
 extern "C" void bssn_oracle_algebra(const double*, const double*, const double*, double, double*);
 extern "C" void bssn_oracle_constraints(const double*, const double*, double*);
 extern "C" void bssn_oracle_algebra_adv(const double*, const double*, const double*, double, double*);
@@ -34,6 +36,7 @@ int main(int argc, char** argv) {
   const bool con = argc > 2 && std::strcmp(argv[2], "con") == 0;
   const bool adv = argc > 2 && std::strcmp(argv[2], "adv") == 0;
   const bool advsame = argc > 2 && std::strcmp(argv[2], "advsame") == 0;
+  const bool split = argc > 2 && std::strcmp(argv[2], "split") == 0;
   const int nout = con ? 4 : 24;
   std::mt19937_64 g(12345);
   std::uniform_real_distribution<double> U(-0.3, 0.3);
@@ -58,6 +61,11 @@ int main(int argc, char** argv) {
     } else if (adv) {
       b200bssn::bssn_rhs_algebra_adv<double>(in, s, prm, eta);
       bssn_oracle_algebra_adv(u, d, par, eta, b);
+    } else if (split) {
+      for (double& x : a) x = NAN;  // every output must be written by exactly one part
+      b200bssn::RhsAlgebraPart<0>::run<double>(in, s, prm, eta);
+      b200bssn::RhsAlgebraPart<1>::run<double>(in, s, prm, eta);
+      bssn_oracle_algebra(u, d, par, eta, b);
     } else if (advsame) {
       for (int k = 0; k < 72; ++k) d[138 + k] = d[k];  // agrad_a_<v> = grad_a_<v>
       bssn_oracle_algebra_adv(u, d, par, eta, a);
@@ -67,7 +75,8 @@ int main(int argc, char** argv) {
       bssn_oracle_algebra(u, d, par, eta, b);
     }
     for (int v = 0; v < nout; ++v) {
-      maxdiff[v] = std::fmax(maxdiff[v], std::fabs(a[v] - b[v]));
+      const double dv = std::fabs(a[v] - b[v]);
+      maxdiff[v] = std::isnan(dv) ? INFINITY : std::fmax(maxdiff[v], dv);  // NaN: unwritten
       maxref[v] = std::fmax(maxref[v], std::fabs(b[v]));
     }
   }

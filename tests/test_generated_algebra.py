@@ -59,3 +59,14 @@ def test_upwind_algebra_reduces_to_the_reference_algebra(algcheck):
                          check=True).stdout
     rel = np.array([float(l.split()[1]) for l in out.strip().splitlines()])
     assert rel.max() < 1e-13, rel
+
+
+def test_split_algebra_matches_oracle(algcheck):
+    """The two-part FP64 algebra (the six At_rhs with the Ricci tensor, then the other 18
+    outputs, each part pruned to the stages it needs and CSE'd on its own) against the
+    oracle's flat C algebra; every output is written by one of the parts."""
+    out = subprocess.run([algcheck, "3000", "split"], capture_output=True, text=True,
+                         check=True).stdout
+    rel = np.array([float(l.split()[1]) for l in out.strip().splitlines()])
+    assert rel.shape == (24,)
+    assert np.isfinite(rel).all() and rel.max() < 1e-13, rel

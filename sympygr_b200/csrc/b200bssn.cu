@@ -925,11 +925,23 @@ int b200bssn_rhs_plan_host(b200bssn_plan* P, double* const* rhs, const double* c
 
 namespace {
 
+// Drop-in calls in flight in this process: a host code may call the drop-in from
+// many threads at once (each with its own context, as the reference's OpenMP block
+// loop calls bssnrhs), and they share the host's cores for their staging copies.
+std::atomic<int> g_dropin_calls{0};
+struct DropinCall {
+  DropinCall() { g_dropin_calls.fetch_add(1); }
+  ~DropinCall() { g_dropin_calls.fetch_sub(1); }
+  DropinCall(const DropinCall&) = delete;
+  DropinCall& operator=(const DropinCall&) = delete;
+};
+
 // Host threads for staging `bytes` of block data: one per 4 MB, at most 8 and at
-// most the host's hardware threads.
+// most this call's share of the host's hardware threads.
 int staging_threads(size_t bytes) {
   const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-  return (int)std::min<size_t>({8, hw, bytes / (4u << 20) + 1});
+  const unsigned share = std::max(1u, hw / (unsigned)std::max(1, g_dropin_calls.load()));
+  return (int)std::min<size_t>({8, share, bytes / (4u << 20) + 1});
 }
 
 // Runs fn(i) for i in [0, n) on up to `threads` host threads (the calling thread
@@ -1103,6 +1115,7 @@ int b200bssn_rhs(b200bssn_ctx* ctx, double* const* rhs, const double* const* u, 
                  const double* pmin, const double* pmax, const uint32_t* sz, uint32_t bflag,
                  const b200bssn_params* prm) {
   b200bssn::host::NvtxRange nvtx_("b200bssn_rhs");
+  const DropinCall call_;
   if (!ctx || !rhs || !u || !pmin || !pmax || !sz || !params_ok(prm))
     return B200BSSN_ERR_INVALID_ARGUMENT;
   for (int v = 0; v < kNumVars; ++v)
@@ -1120,6 +1133,7 @@ int b200bssn_physical_constraints(b200bssn_ctx* ctx, double* const* con, const d
                                   uint32_t offset, const double* pmin, const double* pmax,
                                   const uint32_t* sz, uint32_t bflag, uint32_t precision) {
   b200bssn::host::NvtxRange nvtx_("b200bssn_physical_constraints");
+  const DropinCall call_;
   if (!ctx || !con || !u || !pmin || !pmax || !sz) return B200BSSN_ERR_INVALID_ARGUMENT;
   if (precision != B200BSSN_FP64 && precision != B200BSSN_MIXED) return B200BSSN_ERR_INVALID_ARGUMENT;
   for (int v = 0; v < kNumVars; ++v)

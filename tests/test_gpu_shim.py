@@ -23,14 +23,16 @@ def _driver(tmp_path):
 
 
 @pytest.mark.parametrize("n,bflag,sigma,entry", [(17, 0x00, 0.2, "rhs"), (21, 0x3F, 0.35, "rhs"),
-                                                (19, 0x15, 0.3, "sep")])
+                                                (19, 0x15, 0.3, "sep"), (45, 0x2A, 0.25, "threads")])
 def test_shim_matches_oracle(tmp_path, n, bflag, sigma, entry):
     exe = _driver(tmp_path)
     p0, h = -0.4, 0.8 / n
     u, blk = po.fake_block(n, (p0, p0, p0), h, bflag)
     inp, out = tmp_path / "u.bin", tmp_path / "r.bin"
     u.astype(np.float64).tofile(inp)
-    extra = ["sep"] if entry == "sep" else []
+    # "threads": 4 host threads calling bssnrhs at once, each with the shim's per-thread
+    # context, every result bitwise equal to the first call's
+    extra = [entry] if entry in ("sep", "threads") else []
     subprocess.run([exe, str(inp), str(out), str(n), repr(p0), repr(h), str(bflag), repr(sigma),
                     *extra], check=True)
     got = np.fromfile(out, dtype=np.float64).reshape(24, -1)

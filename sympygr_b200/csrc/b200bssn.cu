@@ -936,6 +936,10 @@ struct DropinCall {
   DropinCall& operator=(const DropinCall&) = delete;
 };
 
+// Blocks whose 24 variables take at most this many bytes go up in one copy and come
+// back in one (the per-copy cost outweighs the ghost planes copied along).
+constexpr size_t kSmallBlockBytes = size_t(8) << 20;
+
 // Host threads for staging `bytes` of block data: one per 4 MB, at most 8 and at
 // most this call's share of the host's hardware threads.
 int staging_threads(size_t bytes) {
@@ -1040,12 +1044,18 @@ int prepare_block(b200bssn_ctx* ctx, const double* const* u, uint32_t offset, co
     ud[v] = ctx->blk_u + v * npad;
     rd[v] = ctx->blk_rhs + v * npad;
   }
-  // each variable goes through the pinned buffer; its upload is queued as soon as
-  // its host copy is done, so the DMA of one variable overlaps the copy of the next
   double* pin = ctx->blk_pin;
   double* dev = ctx->blk_u;
   cudaStream_t s = ctx->stream;
   const size_t bytes = npad * sizeof(double);
+  if (kNumVars * bytes <= kSmallBlockBytes) {
+    // small block: one host copy per variable into the pinned buffer, one upload
+    for (int v = 0; v < kNumVars; ++v) std::memcpy(pin + v * npad, u[v] + offset, bytes);
+    CK(ctx, cudaMemcpyAsync(dev, pin, kNumVars * bytes, cudaMemcpyHostToDevice, s));
+    return B200BSSN_OK;
+  }
+  // each variable goes through the pinned buffer; its upload is queued as soon as
+  // its host copy is done, so the DMA of one variable overlaps the copy of the next
   const cudaError_t e = host_parallel(
       ctx->device, kNumVars, staging_threads(kNumVars * bytes), [=](int v) {
         std::memcpy(pin + v * npad, u[v] + offset, bytes);
@@ -1065,26 +1075,38 @@ int copy_interior_back(b200bssn_ctx* ctx, double* const* dst, double* const* src
   const size_t nx = sz[0], ny = sz[1], nz = sz[2];
   const size_t plane = nx * ny, npad = plane * nz;
   const size_t lo = 3 * plane, n = (nz - 6) * plane;
+  const size_t row = (nx - 6) * sizeof(double);
+  auto scatter = [&](int v) {
+    const double* from = ctx->blk_pin + v * npad;
+    double* to = dst[v] + offset;
+    for (size_t k = 3; k < nz - 3; ++k)
+      for (size_t j = 3; j < ny - 3; ++j) {
+        const size_t at = k * plane + j * nx + 3;
+        std::memcpy(to + at, from + at, row);
+      }
+  };
+  bool contiguous = true;  // the outputs are consecutive arrays of the block buffer
+  for (int v = 1; v < nout; ++v) contiguous = contiguous && src[v] == src[0] + v * npad;
+  if (contiguous && nout * npad * sizeof(double) <= kSmallBlockBytes) {
+    // small block: one download of the whole output, then the row scatter
+    CK(ctx, cudaMemcpyAsync(ctx->blk_pin, src[0], nout * npad * sizeof(double), cudaMemcpyDeviceToHost,
+                            ctx->stream));
+    CK(ctx, cudaStreamSynchronize(ctx->stream));
+    for (int v = 0; v < nout; ++v) scatter(v);
+    return B200BSSN_OK;
+  }
   for (int v = 0; v < nout; ++v) {
     if (!ctx->blk_ev[v]) CK(ctx, cudaEventCreateWithFlags(&ctx->blk_ev[v], cudaEventDisableTiming));
     CK(ctx, cudaMemcpyAsync(ctx->blk_pin + v * npad + lo, src[v] + lo, n * sizeof(double),
                             cudaMemcpyDeviceToHost, ctx->stream));
     CK(ctx, cudaEventRecord(ctx->blk_ev[v], ctx->stream));
   }
-  const double* pin = ctx->blk_pin;
   const cudaEvent_t* ev = ctx->blk_ev;
-  const size_t row = (nx - 6) * sizeof(double);
   const cudaError_t e = host_parallel(
-      ctx->device, nout, staging_threads(nout * n * sizeof(double)), [=](int v) {
+      ctx->device, nout, staging_threads(nout * n * sizeof(double)), [&](int v) {
         const cudaError_t es = cudaEventSynchronize(ev[v]);
         if (es != cudaSuccess) return es;
-        const double* from = pin + v * npad;
-        double* to = dst[v] + offset;
-        for (size_t k = 3; k < nz - 3; ++k)
-          for (size_t j = 3; j < ny - 3; ++j) {
-            const size_t at = k * plane + j * nx + 3;
-            std::memcpy(to + at, from + at, row);
-          }
+        scatter(v);
         return cudaSuccess;
       });
   if (e != cudaSuccess) return fail_cuda(ctx, e, "block download");

@@ -993,6 +993,9 @@ int prepare_block(b200bssn_ctx* ctx, const double* const* u, uint32_t offset, co
                   const double* pmax, const uint32_t* sz, uint32_t bflag, uint32_t precision,
                   const double** ud, double** rd) {
   CK(ctx, cudaSetDevice(ctx->device));
+  // the pinned buffer is free once the context's earlier copies are done (a call
+  // that returned an error may have left some in flight)
+  CK(ctx, cudaStreamSynchronize(ctx->stream));
   b200bssn_block blk;
   blk.offset = 0;
   blk.bflag = bflag;

@@ -55,8 +55,8 @@ BYTES_VARS = 24 * 8
 # large blocks (four 69^3 and one 135^3, one flagged face): `python bench.py
 # --profile-case {mixed,fp64} [--single-pass]` (derivative stage: its two kernels summed;
 # the one-pass kernel with its default 128-slot ring).
-NCU_TRAFFIC_PER_POINT = {"mixed": {"derivs": 377.0 + 653.0, "algebra": 1124.0, "single_pass": 836.0},
-                         "fp64": {"derivs": 576.0 + 1085.0, "algebra": 1897.0}}
+NCU_TRAFFIC_PER_POINT = {"mixed": {"derivs": 375.0 + 646.0, "algebra": 1124.0, "single_pass": 836.0},
+                         "fp64": {"derivs": 580.0 + 1083.0, "algebra": 1897.0}}
 REF_STEP_CAP, REF_WARMUP_CAP = 3, 1  # reference arm: ~32 s per full-batch step on 16 threads
 
 PG_TIMEOUT_S = 120  # process-group timeout under torchrun (N > 1)

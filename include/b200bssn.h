@@ -177,8 +177,9 @@ int b200bssn_rhs_plan_device(b200bssn_plan *plan, double *const *rhs_dev,
 
 /* Batched right-hand side on HOST arrays: uploads the plan's span of every
  * variable, evaluates, downloads the result (ghost handling per
- * prm->ghost_policy).  `n_elems` is the length of each host array.  Blocks until
- * done. */
+ * prm->ghost_policy; PRESERVE brings back only each block's interior, so the
+ * fastest transfers need page-locked host arrays).  `n_elems` is the length of
+ * each host array.  Blocks until done. */
 int b200bssn_rhs_plan_host(b200bssn_plan *plan, double *const *rhs, const double *const *u,
                            uint64_t n_elems, const b200bssn_params *prm);
 

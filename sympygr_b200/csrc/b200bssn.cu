@@ -550,13 +550,16 @@ int b200bssn_plan_create_ex(b200bssn_ctx* ctx, const b200bssn_block* blocks, uin
   // chunks' blocks are disjoint and in increasing offset order.
   {
     std::vector<uint64_t> lo(P->chunks.size(), UINT64_MAX), hi(P->chunks.size(), 0);
+    P->chunk_blocks.assign(P->chunks.size(), {});
     for (size_t c = 0; c < P->chunks.size(); ++c) {
       const ChunkRec& ch = P->chunks[c];
       for (int r = ch.range_begin; r < ch.range_begin + ch.range_count; ++r) {
-        const BlockDev& B = P->blocks[P->units[P->ranges[r].unit].block];
+        const int32_t bi = P->units[P->ranges[r].unit].block;
+        const BlockDev& B = P->blocks[bi];
         const uint64_t np = (uint64_t)B.sz[0] * B.sz[1] * B.sz[2];
         lo[c] = std::min(lo[c], B.offset);
         hi[c] = std::max(hi[c], B.offset + np);
+        if (P->chunk_blocks[c].empty() || P->chunk_blocks[c].back() != bi) P->chunk_blocks[c].push_back(bi);
       }
     }
     bool ok = P->chunks.size() > 1;
@@ -836,6 +839,26 @@ namespace {
 // RHS (s_d2h), with event edges upload(c) -> K1(c) -> K2(c) -> download(c) and
 // K2(c-2) -> K1(c) (scratch reuse).  Uploads, kernels and downloads of different
 // chunks overlap; both copy directions run at once.
+// Interior x-extent (points) from which a block's result comes back as a strided box
+// copy on the ghost-preserving host path (37^3 blocks and up; 13^3 and 21^3 blocks,
+// with rows of 7 and 15 points, come back whole with their ghosts uploaded first).
+constexpr int kBoxCopyMinRow = 24;
+
+// Enqueues the copy of block B's interior box [3, n-3)^3 from the device array `src`
+// to the host array `dst` (both indexed by the caller's element numbering).
+cudaError_t copy_box_d2h(double* dst, const double* src, const BlockDev& B, cudaStream_t s) {
+  const size_t nx = B.sz[0], ny = B.sz[1];
+  cudaMemcpy3DParms cp;
+  std::memset(&cp, 0, sizeof(cp));
+  cp.srcPtr = make_cudaPitchedPtr(const_cast<double*>(src) + B.offset, nx * sizeof(double), nx, ny);
+  cp.dstPtr = make_cudaPitchedPtr(dst + B.offset, nx * sizeof(double), nx, ny);
+  cp.srcPos = make_cudaPos(3 * sizeof(double), 3, 3);
+  cp.dstPos = cp.srcPos;
+  cp.extent = make_cudaExtent((nx - 6) * sizeof(double), ny - 6, B.sz[2] - 6);
+  cp.kind = cudaMemcpyDeviceToHost;
+  return cudaMemcpy3DAsync(&cp, s);
+}
+
 int host_pipelined(b200bssn_plan* P, double* const* rhs, const double* const* u, double* const* rd,
                    const double* const* ud, const b200bssn_params* prm) {
   b200bssn_ctx* ctx = P->ctx;
@@ -843,17 +866,36 @@ int host_pipelined(b200bssn_plan* P, double* const* rhs, const double* const* u,
   AlgebraArgs aa;
   make_args(P, rd, ud, prm, da, aa);
   const size_t nch = P->chunks.size();
+  const bool preserve = prm->ghost_policy == B200BSSN_GHOSTS_PRESERVE;
   cudaStream_t sin = ctx->s_h2d, s1 = ctx->s_deriv, s2 = ctx->s_alg, sout = ctx->s_d2h;
   CK(ctx, cudaMemsetAsync(P->d_counters, 0, 2 * nch * sizeof(int), s1));
   for (size_t ci = 0; ci < nch; ++ci) {
     const uint64_t a = P->part[ci], b = P->part[ci + 1];
     const size_t nb = (size_t)(b - a) * sizeof(double);
+    // PRESERVE: the interior boxes of large blocks come back by strided copies into the
+    // caller's arrays, so their ghost values are never touched; runs of consecutive small
+    // blocks (rows too short for strided copies to pay) go up with the caller's RHS values
+    // and come back whole, so their ghosts return unchanged
+    std::vector<int32_t> boxes;
+    std::vector<std::pair<uint64_t, uint64_t>> runs;
+    if (preserve) {
+      for (const int32_t bi : P->chunk_blocks[ci]) {
+        const BlockDev& B = P->blocks[bi];
+        const uint64_t lo = B.offset, hi = B.offset + (uint64_t)B.sz[0] * B.sz[1] * B.sz[2];
+        if (B.sz[0] - 6 >= kBoxCopyMinRow)
+          boxes.push_back(bi);
+        else if (!runs.empty() && runs.back().second <= lo && lo - runs.back().second < 64)
+          runs.back().second = hi;  // the gap is alignment padding of the caller's arrays
+        else
+          runs.emplace_back(lo, hi);
+      }
+    }
     for (int v = 0; v < kNumVars; ++v) {
       CK(ctx, cudaMemcpyAsync((void*)(ud[v] + a), u[v] + a, nb, cudaMemcpyHostToDevice, sin));
-      if (prm->ghost_policy == B200BSSN_GHOSTS_PRESERVE)
-        CK(ctx, cudaMemcpyAsync(rd[v] + a, rhs[v] + a, nb, cudaMemcpyHostToDevice, sin));
-      else
-        CK(ctx, cudaMemsetAsync(rd[v] + a, 0, nb, sin));
+      if (!preserve) CK(ctx, cudaMemsetAsync(rd[v] + a, 0, nb, sin));
+      for (const auto& r : runs)
+        CK(ctx, cudaMemcpyAsync(rd[v] + r.first, rhs[v] + r.first, (r.second - r.first) * sizeof(double),
+                                cudaMemcpyHostToDevice, sin));
     }
     CK(ctx, cudaEventRecord(P->ev_in[ci], sin));
     CK(ctx, cudaStreamWaitEvent(s1, P->ev_in[ci], 0));
@@ -861,8 +903,17 @@ int host_pipelined(b200bssn_plan* P, double* const* rhs, const double* const* u,
     const int rc = enqueue_chunk(P, da, aa, ci, (int)(ci & 1), s1, s2, nullptr);
     if (rc != B200BSSN_OK) return rc;
     CK(ctx, cudaStreamWaitEvent(sout, P->ev_alg[ci], 0));
-    for (int v = 0; v < kNumVars; ++v)
-      CK(ctx, cudaMemcpyAsync(rhs[v] + a, rd[v] + a, nb, cudaMemcpyDeviceToHost, sout));
+    if (preserve) {
+      for (const int32_t bi : boxes)
+        for (int v = 0; v < kNumVars; ++v) CK(ctx, copy_box_d2h(rhs[v], rd[v], P->blocks[bi], sout));
+      for (const auto& r : runs)
+        for (int v = 0; v < kNumVars; ++v)
+          CK(ctx, cudaMemcpyAsync(rhs[v] + r.first, rd[v] + r.first, (r.second - r.first) * sizeof(double),
+                                  cudaMemcpyDeviceToHost, sout));
+    } else {
+      for (int v = 0; v < kNumVars; ++v)
+        CK(ctx, cudaMemcpyAsync(rhs[v] + a, rd[v] + a, nb, cudaMemcpyDeviceToHost, sout));
+    }
   }
   CK(ctx, cudaStreamSynchronize(sout));
   CK(ctx, cudaStreamSynchronize(s1));

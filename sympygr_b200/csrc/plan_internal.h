@@ -77,6 +77,7 @@ struct b200bssn_plan {
   // per chunk, when chunks hold whole blocks in increasing offset order
   bool host_pipeline = false;
   std::vector<uint64_t> part;
+  std::vector<std::vector<int32_t>> chunk_blocks;  // per chunk: its blocks (host pipeline)
   std::vector<cudaEvent_t> ev_in;  // per chunk: upload done
   int tile_y = b200bssn::kTileY;      // tile height of the derivative kernels (4, 8 or 16)
   int deriv_regs = 0;                 // register split variant of the derivative kernels

@@ -161,7 +161,8 @@ def test_chunking_is_bitwise_invariant(ctx):
 @pytest.mark.parametrize("chunk_points", [0, 3000])  # 3000: several chunks, pipelined copies
 @pytest.mark.parametrize("policy", [sg.GHOSTS_PRESERVE, sg.GHOSTS_ZERO])
 def test_batch_host_ghost_policy(ctx, oracle_lib, policy, chunk_points):
-    u, blocks, total = _fake_batch(BATCH[:4], seed=5)
+    # small blocks and two whose interiors come back as strided boxes under PRESERVE
+    u, blocks, total = _fake_batch(BATCH[:4] + [(37, 0x00), (45, 0x2A)], seed=5)
     plan = sg.Plan(ctx, blocks, sg.FP64, chunk_points)
     assert chunk_points == 0 or plan.launches >= 6
     rhs = np.full_like(u, 7.0)

@@ -891,8 +891,9 @@ int host_pipelined(b200bssn_plan* P, double* const* rhs, const double* const* u,
       }
     }
     for (int v = 0; v < kNumVars; ++v) {
+      // (ZERO: st_rhs was cleared once, before the first chunk; the kernels write
+      // interior points only)
       CK(ctx, cudaMemcpyAsync((void*)(ud[v] + a), u[v] + a, nb, cudaMemcpyHostToDevice, sin));
-      if (!preserve) CK(ctx, cudaMemsetAsync(rd[v] + a, 0, nb, sin));
       for (const auto& r : runs)
         CK(ctx, cudaMemcpyAsync(rd[v] + r.first, rhs[v] + r.first, (r.second - r.first) * sizeof(double),
                                 cudaMemcpyHostToDevice, sin));
@@ -943,6 +944,7 @@ int b200bssn_rhs_plan_host(b200bssn_plan* P, double* const* rhs, const double* c
     CK(ctx, cudaMalloc((void**)&P->st_u, (size_t)kNumVars * len * sizeof(double)));
     CK(ctx, cudaMalloc((void**)&P->st_rhs, (size_t)kNumVars * len * sizeof(double)));
     P->st_len = len;
+    P->st_rhs_zeroed = false;
   }
   cudaStream_t s = ctx->stream;
   const double* ud[kNumVars];
@@ -953,6 +955,12 @@ int b200bssn_rhs_plan_host(b200bssn_plan* P, double* const* rhs, const double* c
     ud[v] = P->st_u + (size_t)v * len - P->span_lo;
     rd[v] = P->st_rhs + (size_t)v * len - P->span_lo;
   }
+  if (prm->ghost_policy == B200BSSN_GHOSTS_PRESERVE) {
+    P->st_rhs_zeroed = false;  // the caller's RHS values go into st_rhs below
+  } else if (!P->st_rhs_zeroed) {
+    CK(ctx, cudaMemsetAsync(P->st_rhs, 0, (size_t)kNumVars * bytes, P->host_pipeline ? ctx->s_h2d : s));
+    P->st_rhs_zeroed = true;
+  }
   if (P->host_pipeline) return host_pipelined(P, rhs, u, rd, ud, prm);
   for (int v = 0; v < kNumVars; ++v) {
     CK(ctx, cudaMemcpyAsync(P->st_u + (size_t)v * len, u[v] + P->span_lo, bytes,
@@ -960,8 +968,6 @@ int b200bssn_rhs_plan_host(b200bssn_plan* P, double* const* rhs, const double* c
     if (prm->ghost_policy == B200BSSN_GHOSTS_PRESERVE)
       CK(ctx, cudaMemcpyAsync(P->st_rhs + (size_t)v * len, rhs[v] + P->span_lo, bytes,
                               cudaMemcpyHostToDevice, s));
-    else
-      CK(ctx, cudaMemsetAsync(P->st_rhs + (size_t)v * len, 0, bytes, s));
   }
   int rc = launch_plan(P, rd, ud, prm, s);
   if (rc != B200BSSN_OK) return rc;

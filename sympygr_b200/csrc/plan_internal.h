@@ -100,6 +100,10 @@ struct b200bssn_plan {
   double* st_u = nullptr;
   double* st_rhs = nullptr;
   uint64_t st_len = 0;
+  // st_rhs holds zeros wherever no kernel writes (ghost points, gaps between blocks):
+  // the kernels write interior points only, so one clearing lasts until a
+  // ghost-preserving call puts the caller's values there
+  bool st_rhs_zeroed = false;
 };
 
 namespace b200bssn {

@@ -185,6 +185,31 @@ def test_batch_host_ghost_policy(ctx, oracle_lib, policy, chunk_points):
     plan.close()
 
 
+@pytest.mark.parametrize("chunk_points", [0, 3000])
+def test_batch_host_ghost_policy_sequence(ctx, chunk_points):
+    """One plan alternating the two policies: a ghost-preserving call puts the caller's
+    RHS values into the plan's device staging, so the next zeroing call must clear them
+    again; repeated zeroing calls keep zeros; the interiors never change."""
+    u, blocks, total = _fake_batch(BATCH[:4] + [(37, 0x00)], seed=9)
+    plan = sg.Plan(ctx, blocks, sg.FP64, chunk_points)
+    ghost = np.ones(total, dtype=bool)
+    for b in blocks:
+        ghost[b.offset:b.offset + b.npad] &= ~wl.interior_mask(b).ravel()
+    ref = None
+    for policy, fill in ((sg.GHOSTS_ZERO, 3.0), (sg.GHOSTS_PRESERVE, 7.0), (sg.GHOSTS_ZERO, 5.0),
+                         (sg.GHOSTS_ZERO, 6.0), (sg.GHOSTS_PRESERVE, 8.0)):
+        rhs = np.full_like(u, fill)
+        plan.rhs_host(list(rhs), list(u), total, sg.Params.make(ko_sigma=0.1, ghost_policy=policy))
+        lo = min(b.offset for b in blocks)
+        g = rhs[:, lo:][:, ghost[lo:]]
+        assert np.all(g == (fill if policy == sg.GHOSTS_PRESERVE else 0.0)), (policy, fill)
+        inner = rhs[:, ~ghost]
+        if ref is None:
+            ref = inner.copy()
+        assert np.array_equal(inner, ref)
+    plan.close()
+
+
 @pytest.mark.parametrize("maker", ["fake", "sines", "bl"])
 def test_mixed_precision_error(ctx, oracle_lib, maker):
     if maker == "fake":

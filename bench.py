@@ -128,7 +128,9 @@ def _env_int(k, d):
 
 
 class ClockSampler:
-    """nvidia-smi clocks/throttle sampling during the timed region."""
+    """nvidia-smi clocks/throttle sampling during the timed region: started before the
+    warm-up (nvidia-smi takes a moment to begin), every 100 ms, and only the samples
+    taken between begin() and end() count (all of them if none fell there)."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -139,12 +141,13 @@ class ClockSampler:
         self.proc = None
         self.lines = []
         self.t = None
+        self.window = (None, None)
 
     def start(self):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except Exception:
             self.proc = None
             return
@@ -153,7 +156,13 @@ class ClockSampler:
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.monotonic(), line.strip()))
+
+    def begin(self):
+        self.window = (time.monotonic(), None)
+
+    def end(self):
+        self.window = (self.window[0], time.monotonic())
 
     def stop(self):
         if self.proc is None:
@@ -165,8 +174,11 @@ class ClockSampler:
             self.proc.kill()
         if self.t:
             self.t.join(timeout=2)
+        t0, t1 = self.window
+        inside = [ln for t, ln in self.lines if t0 is not None and t1 is not None and t0 <= t <= t1]
+        lines = inside or [ln for _, ln in self.lines]
         sm, smax, reasons, power = [], None, set(), []
-        for ln in self.lines:
+        for ln in lines:
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 9:
                 continue
@@ -181,7 +193,7 @@ class ClockSampler:
                 if val.lower().startswith("active"):
                     reasons.add(name)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
-                "reasons": sorted(reasons), "samples": len(sm),
+                "reasons": sorted(reasons), "samples": len(sm), "in_timed_region": bool(inside),
                 "power_w_max": max(power) if power else None}
 
 
@@ -642,14 +654,16 @@ def main():
         barrier()
         return max_over_ranks(e0.elapsed_time(e1), dist) / k
 
+    clocks = ClockSampler(local_rank)
+    clocks.start()
     for prec in (sg.MIXED, sg.FP64):
         for _ in range(args.warmup):
             plans[prec].rhs_device(R, U, params[prec])
     torch.cuda.synchronize()
 
-    clocks = ClockSampler(local_rank)
-    clocks.start()
+    clocks.begin()
     ms_mixed = timed(sg.MIXED, args.steps)
+    clocks.end()
     clock_info = clocks.stop()
     ms_fp64 = timed(sg.FP64, args.steps)
     for p in plans.values():

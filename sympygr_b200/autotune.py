@@ -21,8 +21,10 @@ for every candidate of
 It writes the per-class table and choice to JSON.  ``tuned_plan`` builds a plan for
 any block list from such a table: each block gets its class's slab depth
 (b200bssn_plan_options.block_slab_depth); the tile shape, register split and CTA
-count, plan-wide knobs, are the choice of the class holding the most points.  The run
-ends with the whole batch timed with the default knobs and with the tuned ones.
+count are plan-wide knobs.  They are settled on the whole batch: the default plan, the
+per-class depths with the default plan-wide knobs, and the per-class depths with the
+knobs of the class holding the most points are timed, and the table keeps the fastest
+(so a class's win inside the timing noise cannot cost the other classes).
 
     python -m sympygr_b200.autotune --precision mixed --json tune_mixed.json
 """
@@ -71,8 +73,10 @@ KERNEL_VARIANTS = [(8, 1, 1), (4, 1, 1), (16, 1, 1), (8, 2, 1), (8, 3, 1), (16, 
 
 
 def tuned_plan(ctx, blocks, precision, table, chunk_points: int = 0):
-    """A plan whose blocks use their size class's tuned slab depth and the plan-wide
-    knobs of the class holding the most points."""
+    """A plan whose blocks use their size class's tuned slab depth and the table's
+    plan-wide knobs (the default plan where the table found the tuned one no faster)."""
+    if table.get("use_default_plan"):
+        return capi.Plan(ctx, blocks, precision, chunk_points)
     choice = {int(k): v for k, v in table["choice"].items()}
     depths = [choice.get(b.sz[2], {}).get("slab_depth", 0) for b in blocks]
     return capi.Plan(ctx, blocks, precision, chunk_points, deriv_ctas_per_sm=table["deriv_ctas_per_sm"],
@@ -124,20 +128,31 @@ def main(argv=None):
             best_points = (pts, best)
         del u, rhs
         torch.cuda.empty_cache()
-    for k in ("deriv_ctas_per_sm", "tile_y", "deriv_regs", "points_per_thread"):
-        table[k] = best_points[1][k]
-    # the whole batch: default knobs against the tuned table
+    # the whole batch settles the plan-wide knobs: the default plan, the per-class depths
+    # with the default knobs, and the per-class depths with the knobs of the class
+    # holding the most points
+    knobs = ("deriv_ctas_per_sm", "tile_y", "deriv_regs", "points_per_thread")
     u, blocks = wl.two_puncture_batch_torch(wl.BATCH_SIZES, counts, seed=0, device="cuda")
     rhs = torch.zeros_like(u)
     pts = sum(b.ninterior for b in blocks)
     plan = capi.Plan(ctx, blocks, prec)
     ms_default = time_plan(plan, list(rhs), list(u), prm, args.reps)
     plan.close()
-    plan = tuned_plan(ctx, blocks, prec, table)
-    ms_tuned = time_plan(plan, list(rhs), list(u), prm, args.reps)
-    plan.close()
+    candidates = {"default_knobs": {k: 0 for k in knobs},
+                  "class_knobs": {k: best_points[1][k] for k in knobs}}
+    timed = {}
+    for name, kn in candidates.items():
+        table.update(kn)
+        plan = tuned_plan(ctx, blocks, prec, table)
+        timed[name] = time_plan(plan, list(rhs), list(u), prm, args.reps)
+        plan.close()
+    pick = min(timed, key=timed.get)
+    table.update(candidates[pick])
+    table["use_default_plan"] = ms_default <= timed[pick]  # the tuned depths did not pay
     table["batch"] = {"points": pts, "default_mpts_per_s": pts / ms_default / 1e3,
-                      "tuned_mpts_per_s": pts / ms_tuned / 1e3}
+                      "depths_default_knobs_mpts_per_s": pts / timed["default_knobs"] / 1e3,
+                      "depths_class_knobs_mpts_per_s": pts / timed["class_knobs"] / 1e3,
+                      "tuned_mpts_per_s": pts / min(ms_default, timed[pick]) / 1e3, "plan_wide": pick}
     print(json.dumps({"choice": table["choice"], "batch": table["batch"],
                       "plan_wide": {k: table[k] for k in ("deriv_ctas_per_sm", "tile_y", "deriv_regs",
                                                           "points_per_thread")}}),

@@ -197,6 +197,47 @@ def _ptr_table(arrays: Sequence, n: int = NUM_VARS) -> ctypes.Array:
     return (ctypes.c_void_p * n)(*ptrs)
 
 
+class _TorchOrder:
+    """Orders a library call on `stream` with torch's work on the tensors passed.
+
+    torch fills and reads its tensors on its current stream, and the library's
+    streams (the context stream included, created non-blocking) do not synchronise
+    with it: without this, an evaluation can start before torch has finished writing
+    its inputs (or zeroing its outputs, overwriting results written meanwhile), and
+    torch can read results before the evaluation wrote them.  Entering makes `stream`
+    wait for everything torch has queued on the tensors' device so far; leaving makes
+    torch's current stream wait for the call.  Calls given only numpy arrays or raw
+    pointers are left as they are."""
+
+    def __init__(self, stream: int, *groups):
+        self.stream, self.t = stream, None
+        for g in groups:
+            for a in (g if g is not None else ()):
+                if not isinstance(a, (np.ndarray, int)) and getattr(a, "is_cuda", False):
+                    self.t = a
+                    break
+            if self.t is not None:
+                break
+
+    def __enter__(self):
+        if self.t is not None:
+            import torch
+
+            ev = torch.cuda.Event()
+            ev.record(torch.cuda.current_stream(self.t.device))
+            torch.cuda.ExternalStream(self.stream, device=self.t.device).wait_event(ev)
+        return self
+
+    def __exit__(self, exc_type, exc, tb):
+        if self.t is not None and exc_type is None:
+            import torch
+
+            ev = torch.cuda.Event()
+            ev.record(torch.cuda.ExternalStream(self.stream, device=self.t.device))
+            torch.cuda.current_stream(self.t.device).wait_event(ev)
+        return False
+
+
 NOALLOC_MAX_POINTS = 32768
 NUM_CONSTRAINTS = 4  # ham, mom0, mom1, mom2
 
@@ -341,10 +382,12 @@ class Plan:
 
     def rhs_device(self, rhs, u, params: Params, stream: int = 0):
         """Batched RHS on device arrays (torch CUDA tensors or raw pointers);
-        asynchronous on `stream` (0: the context stream)."""
-        _check(load().b200bssn_rhs_plan_device(self.handle, _ptr_table(rhs), _ptr_table(u),
-                                               ctypes.byref(params), ctypes.c_void_p(stream or None)),
-               "b200bssn_rhs_plan_device", self.ctx)
+        asynchronous on `stream` (0: the context stream), ordered after torch's work
+        on the tensors passed and before torch's later work (_TorchOrder)."""
+        with _TorchOrder(stream or self.ctx.stream, rhs, u):
+            _check(load().b200bssn_rhs_plan_device(self.handle, _ptr_table(rhs), _ptr_table(u),
+                                                   ctypes.byref(params), ctypes.c_void_p(stream or None)),
+                   "b200bssn_rhs_plan_device", self.ctx)
 
     def constraints_device(self, u, con=None, block_norms=None, stream: int = 0):
         """Constraints of every block on device arrays: `con` (4 device arrays or
@@ -357,10 +400,11 @@ class Plan:
             if block_norms.numel() < 8 * self.nblocks or str(block_norms.dtype) != "torch.float64":
                 raise ValueError("block_norms must hold nblocks*8 float64")
             npt = block_norms.data_ptr()
-        _check(load().b200bssn_constraints_plan_device(self.handle, cp, _ptr_table(u),
-                                                       ctypes.c_void_p(npt),
-                                                       ctypes.c_void_p(stream or None)),
-               "b200bssn_constraints_plan_device", self.ctx)
+        with _TorchOrder(stream or self.ctx.stream, u, con, [block_norms] if block_norms is not None else None):
+            _check(load().b200bssn_constraints_plan_device(self.handle, cp, _ptr_table(u),
+                                                           ctypes.c_void_p(npt),
+                                                           ctypes.c_void_p(stream or None)),
+                   "b200bssn_constraints_plan_device", self.ctx)
 
     def check_finite(self, arrays, stream: int = 0):
         """NaN/Inf guard over the interior points of the plan's blocks in the given
@@ -368,8 +412,9 @@ class Plan:
         offending element index."""
         n = len(arrays)
         bad = ctypes.c_uint64()
-        rc = load().b200bssn_check_finite(self.handle, _ptr_table(arrays, n), n, ctypes.byref(bad),
-                                          ctypes.c_void_p(stream or None))
+        with _TorchOrder(stream or self.ctx.stream, arrays):
+            rc = load().b200bssn_check_finite(self.handle, _ptr_table(arrays, n), n, ctypes.byref(bad),
+                                              ctypes.c_void_p(stream or None))
         if rc == -6:
             return int(bad.value)
         _check(rc, "b200bssn_check_finite", self.ctx)
@@ -378,9 +423,10 @@ class Plan:
     def profile(self, rhs, u, params: Params):
         """One evaluation with per-launch events: (derivative ms, algebra ms)."""
         d, a = ctypes.c_double(), ctypes.c_double()
-        _check(load().b200bssn_plan_profile(self.handle, _ptr_table(rhs), _ptr_table(u),
-                                            ctypes.byref(params), ctypes.byref(d), ctypes.byref(a)),
-               "b200bssn_plan_profile", self.ctx)
+        with _TorchOrder(self.ctx.stream, rhs, u):
+            _check(load().b200bssn_plan_profile(self.handle, _ptr_table(rhs), _ptr_table(u),
+                                                ctypes.byref(params), ctypes.byref(d), ctypes.byref(a)),
+                   "b200bssn_plan_profile", self.ctx)
         return d.value, a.value
 
     def rhs_host(self, rhs, u, n_elems: int, params: Params):
@@ -415,8 +461,9 @@ class RK4:
 
     def init(self, u, stream: int = 0):
         """Copy the state (ghosts included) into both stage states."""
-        _check(load().b200bssn_rk4_init(self.handle, _ptr_table(u), ctypes.c_void_p(stream or None)),
-               "b200bssn_rk4_init", self.plan.ctx)
+        with _TorchOrder(stream or self.plan.ctx.stream, u):
+            _check(load().b200bssn_rk4_init(self.handle, _ptr_table(u), ctypes.c_void_p(stream or None)),
+                   "b200bssn_rk4_init", self.plan.ctx)
 
     def stage_state(self, stage: int):
         """Device pointers (24 ints; 0 for stage 0) of the state stage `stage` reads."""
@@ -426,24 +473,28 @@ class RK4:
         return [int(p or 0) for p in out]
 
     def stage(self, stage: int, u, dt: float, params: Params, stream: int = 0):
-        _check(load().b200bssn_rk4_stage(self.handle, stage, _ptr_table(u), float(dt),
-                                         ctypes.byref(params), ctypes.c_void_p(stream or None)),
-               "b200bssn_rk4_stage", self.plan.ctx)
+        with _TorchOrder(stream or self.plan.ctx.stream, u):
+            _check(load().b200bssn_rk4_stage(self.handle, stage, _ptr_table(u), float(dt),
+                                             ctypes.byref(params), ctypes.c_void_p(stream or None)),
+                   "b200bssn_rk4_stage", self.plan.ctx)
 
     def step(self, u, dt: float, params: Params, stream: int = 0):
-        _check(load().b200bssn_rk4_step(self.handle, _ptr_table(u), float(dt), ctypes.byref(params),
-                                        ctypes.c_void_p(stream or None)),
-               "b200bssn_rk4_step", self.plan.ctx)
+        with _TorchOrder(stream or self.plan.ctx.stream, u):
+            _check(load().b200bssn_rk4_step(self.handle, _ptr_table(u), float(dt), ctypes.byref(params),
+                                            ctypes.c_void_p(stream or None)),
+                   "b200bssn_rk4_step", self.plan.ctx)
 
     def capture(self, u, dt: float, params: Params, steps: int = 1):
         """Capture `steps` full steps into a CUDA graph (replay with ``launch``)."""
+        self._graph_arrays = list(u)
         _check(load().b200bssn_rk4_graph_capture(self.handle, _ptr_table(u), float(dt),
                                                  ctypes.byref(params), int(steps)),
                "b200bssn_rk4_graph_capture", self.plan.ctx)
 
     def launch(self, stream: int = 0):
-        _check(load().b200bssn_rk4_graph_launch(self.handle, ctypes.c_void_p(stream or None)),
-               "b200bssn_rk4_graph_launch", self.plan.ctx)
+        with _TorchOrder(stream or self.plan.ctx.stream, getattr(self, "_graph_arrays", None)):
+            _check(load().b200bssn_rk4_graph_launch(self.handle, ctypes.c_void_p(stream or None)),
+                   "b200bssn_rk4_graph_launch", self.plan.ctx)
 
     @property
     def graph_steps(self) -> int:
